@@ -1,0 +1,155 @@
+/*
+ * mela.h -- C ABI of the B200 (sm_100a) GF(2) linear-algebra library.
+ *
+ * Drop-in boundary for the six MEX functions of HCPhy/mex_linear_algebra:
+ *
+ *   reference gateway (file:line of its mexFunction)     replaced by
+ *   mela_matmul_gf2   src/mela_matmul_gf2.c:72-211       mela_matmul_gf2()
+ *   mela_matmul_m4ri  src/mela_matmul_m4ri.c:140-251     mela_matmul_m4ri()
+ *   mela_rank_gf2     src/mela_rank_gf2.c:126-186        mela_rank_gf2()
+ *   mela_rank_m4ri    src/mela_rank_m4ri.c:286-341       mela_rank_m4ri()
+ *   mela_null_gf2     src/mela_null_gf2.c:142-281        mela_null_gf2()
+ *   mela_null_m4ri    src/mela_null_m4ri.c:251-408       mela_null_m4ri()
+ *
+ * The host entry points take MATLAB-layout (column-major) logical or double
+ * arrays in host memory, exactly what a MEX gateway receives, and return
+ * status codes instead of long-jumping; the MEX gateways in
+ * mex_linear_algebra_b200/mex/ map each status to the reference's own error
+ * text.  The mela_dev_* entry points work on device-resident bit-packed
+ * matrices and are stream-ordered.
+ *
+ * Packed layout: row-major uint64_t words, bit j of row i in word
+ * i*ld + j/64 at bit j%64 (the reference's convention,
+ * src/mela_matmul_gf2.c:33-36).  Bits past the last column are zero.
+ *
+ * Every result is bit-exact: products, ranks and null-space bases equal the
+ * reference's on every input.  Nothing is computed on the CPU.
+ */
+#ifndef MELA_H
+#define MELA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MELA_OK = 0,
+    MELA_ERR_INVALID = 1,      /* bad pointer / size / variant */
+    MELA_ERR_SPARSE = 2,       /* sparse input where the reference rejects it */
+    MELA_ERR_DIM = 3,          /* inner dimensions disagree */
+    MELA_ERR_TYPE = 4,         /* input neither logical nor double */
+    MELA_ERR_NOMEM = 5,        /* device or host allocation failed */
+    MELA_ERR_CUDA = 6,         /* CUDA runtime error (see mela_last_error) */
+    MELA_ERR_TIMEOUT = 7,      /* a bounded device wait ran out */
+    MELA_ERR_UNSUPPORTED = 8,  /* no sm_100 device, or size beyond a limit */
+    MELA_ERR_NO_DEVICE = 9     /* no CUDA device visible */
+} mela_status;
+
+/* Element kinds of a MATLAB array as the gateways see it. */
+typedef enum {
+    MELA_KIND_LOGICAL = 0,  /* mxLogical, 1 byte, nonzero = 1 */
+    MELA_KIND_DOUBLE = 1,   /* double, read as ((int)x) & 1 */
+    MELA_KIND_OTHER = 2     /* any other class: rejected like the reference */
+} mela_kind;
+
+/* A MATLAB array handed to a gateway: column-major, rows x cols. */
+typedef struct {
+    int32_t kind;     /* mela_kind */
+    int32_t sparse;   /* nonzero if the MATLAB array is sparse */
+    int64_t rows;
+    int64_t cols;
+    const void *data; /* host pointer, rows*cols elements */
+} mela_host_matrix;
+
+/* Product variants (the autotuned choice decides only how, never what). */
+typedef enum {
+    MELA_GEMM_AUTO = 0,
+    MELA_GEMM_PLAIN = 1,  /* bit-packed AND + popcount parity on CUDA cores */
+    MELA_GEMM_M4RI = 2,   /* Four-Russians tables in shared memory */
+    MELA_GEMM_TC = 3      /* tcgen05 kind::i8 tensor cores, parity of the s32 sum */
+} mela_gemm_variant;
+
+/* ------------------------------------------------------------------ */
+/* library                                                             */
+/* ------------------------------------------------------------------ */
+int mela_version(void);
+const char *mela_status_string(mela_status s);
+/* Detail text of the last failure on the calling thread. */
+const char *mela_last_error(void);
+/* Device-side error bits (timeouts of bounded waits); `clear` resets them. */
+mela_status mela_device_error_flags(uint32_t *flags, int clear);
+
+/* ------------------------------------------------------------------ */
+/* host entry points (MATLAB layout in, MATLAB layout out)              */
+/* ------------------------------------------------------------------ */
+
+/* C = A*B over GF(2).  C is rows(A) x cols(B) logical, column-major,
+ * caller-allocated (all bytes written).  Validation order and failure
+ * classes follow src/mela_matmul_gf2.c:75-88: sparse -> MELA_ERR_SPARSE,
+ * inner dimension mismatch -> MELA_ERR_DIM, other classes -> MELA_ERR_TYPE. */
+mela_status mela_matmul_gf2(const mela_host_matrix *A, const mela_host_matrix *B,
+                            uint8_t *C);
+/* Same result through the Four-Russians kernel (src/mela_matmul_m4ri.c). */
+mela_status mela_matmul_m4ri(const mela_host_matrix *A, const mela_host_matrix *B,
+                             uint8_t *C);
+
+/* Host-resident packed product (copies in, computes, copies out). */
+mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, const uint64_t *B,
+                                    int64_t ldb, uint64_t *C, int64_t ldc, int64_t m,
+                                    int64_t k, int64_t n, int32_t variant);
+
+/* ------------------------------------------------------------------ */
+/* device entry points (packed, stream-ordered)                         */
+/* ------------------------------------------------------------------ */
+
+/* Seeded Bernoulli(1/2) packed matrix: word w of row i is output number
+ * i*ceil(n/64)+w of a counter-based splitmix64 stream keyed by
+ * (seed, stream_id); bits past column n are zero. */
+mela_status mela_dev_rand_dense(uint64_t seed, uint64_t stream_id, int64_t m, int64_t n,
+                                uint64_t *d_out, int64_t ld, void *stream);
+
+/* Column-major logical (kind 0) or double (kind 1) m x n -> packed rows.
+ * Replaces pack_rows_logical/pack_rows_double (src/mela_matmul_gf2.c:42-69)
+ * and the inline packs of the other gateways. */
+mela_status mela_dev_pack(int32_t kind, int64_t m, int64_t n, const void *d_in,
+                          uint64_t *d_out, int64_t ld, void *stream);
+/* Packed rows -> column-major logical bytes (src/mela_matmul_gf2.c:193-205). */
+mela_status mela_dev_unpack(const uint64_t *d_in, int64_t ld, int64_t m, int64_t n,
+                            uint8_t *d_out, void *stream);
+/* Bit transpose: out (cols x rows) = in (rows x cols)^T. */
+mela_status mela_dev_transpose(const uint64_t *d_in, int64_t ld_in, int64_t rows,
+                               int64_t cols, uint64_t *d_out, int64_t ld_out, void *stream);
+
+/* Workspace bytes mela_dev_matmul needs for this variant and shape. */
+size_t mela_matmul_workspace_size(int32_t variant, int64_t m, int64_t k, int64_t n);
+/* C = A*B mod 2 on packed device matrices (A m x k, B k x n, C m x n).
+ * Replaces the product loops of src/mela_matmul_gf2.c:111-208 and
+ * src/mela_matmul_m4ri.c:179-248.  `workspace` must hold
+ * mela_matmul_workspace_size() bytes (may be NULL when that is 0). */
+mela_status mela_dev_matmul(int32_t variant, const uint64_t *dA, int64_t lda,
+                            const uint64_t *dB, int64_t ldb, uint64_t *dC, int64_t ldc,
+                            int64_t m, int64_t k, int64_t n, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
+/* The two halves of mela_dev_matmul, for callers that overlap or time them
+ * separately: operand preparation into the workspace (B transposed; for the
+ * tensor-core form also the 0/1 byte expansion of A and B^T), then the
+ * product kernel over the prepared operands.  Same arguments and workspace
+ * as mela_dev_matmul; run must follow prepare on the same stream. */
+mela_status mela_dev_matmul_prepare(int32_t variant, const uint64_t *dA, int64_t lda,
+                                    const uint64_t *dB, int64_t ldb, int64_t m, int64_t k,
+                                    int64_t n, void *workspace, size_t workspace_bytes,
+                                    void *stream);
+mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, int64_t lda,
+                                const uint64_t *dB, int64_t ldb, uint64_t *dC, int64_t ldc,
+                                int64_t m, int64_t k, int64_t n, void *workspace,
+                                size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MELA_H */

@@ -1,0 +1,81 @@
+"""ctypes binding of ``libmela_b200.so`` (the C ABI declared in include/mela.h).
+
+The library is loaded from the package directory; if it is missing the
+import fails loudly -- there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmela_b200.so")
+
+# mela_status
+OK, ERR_INVALID, ERR_SPARSE, ERR_DIM, ERR_TYPE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, \
+    ERR_UNSUPPORTED, ERR_NO_DEVICE = range(10)
+# mela_kind
+KIND_LOGICAL, KIND_DOUBLE, KIND_OTHER = 0, 1, 2
+# mela_gemm_variant
+GEMM_AUTO, GEMM_PLAIN, GEMM_M4RI, GEMM_TC = 0, 1, 2, 3
+GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc": GEMM_TC}
+
+
+class HostMatrix(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("sparse", C.c_int32), ("rows", C.c_int64),
+                ("cols", C.c_int64), ("data", C.c_void_p)]
+
+
+# name -> (restype, argtypes); the list of every exported entry point
+_i64, _u64, _i32, _u32, _vp, _sz = C.c_int64, C.c_uint64, C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t
+_st = C.c_int
+SIGNATURES = {
+    "mela_version": (C.c_int, []),
+    "mela_status_string": (C.c_char_p, [_st]),
+    "mela_last_error": (C.c_char_p, []),
+    "mela_device_error_flags": (_st, [C.POINTER(_u32), C.c_int]),
+    "mela_matmul_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
+    "mela_matmul_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
+    "mela_matmul_packed_host": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i32]),
+    "mela_dev_rand_dense": (_st, [_u64, _u64, _i64, _i64, _vp, _i64, _vp]),
+    "mela_dev_pack": (_st, [_i32, _i64, _i64, _vp, _vp, _i64, _vp]),
+    "mela_dev_unpack": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
+    "mela_dev_transpose": (_st, [_vp, _i64, _i64, _i64, _vp, _i64, _vp]),
+    "mela_matmul_workspace_size": (_sz, [_i32, _i64, _i64, _i64]),
+    "mela_dev_matmul": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "mela_dev_matmul_prepare": (_st, [_i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "mela_dev_matmul_run": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA library first "
+                "(python -m mex_linear_algebra_b200.build); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MelaError(RuntimeError):
+    """A failed library call: ``status`` is the mela_status code."""
+
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        self.detail = detail
+        msg = lib().mela_status_string(status).decode()
+        super().__init__(f"{msg}: {detail}" if detail else msg)
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise MelaError(status, lib().mela_last_error().decode())

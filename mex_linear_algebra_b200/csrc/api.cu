@@ -1,0 +1,475 @@
+// api.cu -- C host layer behind the C ABI (include/mela.h).
+//
+// Host entry points mirror the reference MEX gateways' semantics (input
+// validation order, logical/double reading, MATLAB column-major layout) and
+// run every computation on the GPU: host arrays are copied in, packed,
+// processed and unpacked by kernels, and copied out.  Device entry points
+// are stream-ordered and never synchronise.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "mela_common.cuh"
+#include "mela_internal.h"
+#include "mela_host.h"
+
+namespace mela {
+
+// ---------------------------------------------------------------- errors
+static thread_local char t_err[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_err, sizeof t_err, fmt, ap);
+    va_end(ap);
+}
+
+mela_status cuda_status(cudaError_t e, const char *what)
+{
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return MELA_ERR_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return MELA_ERR_NO_DEVICE;
+    return MELA_ERR_CUDA;
+}
+
+__device__ u32 g_device_error;
+
+static constexpr int kMaxDevices = 64;
+static std::mutex g_dev_mu;
+static u32 *g_err_addr[kMaxDevices];
+static int g_sms[kMaxDevices];
+
+static int current_device()
+{
+    int d = 0;
+    cudaGetDevice(&d);
+    return (d >= 0 && d < kMaxDevices) ? d : 0;
+}
+
+u32 *device_error_word()
+{
+    int d = current_device();
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    if (!g_err_addr[d]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_device_error) == cudaSuccess) g_err_addr[d] = (u32 *)p;
+    }
+    return g_err_addr[d];
+}
+
+int sm_count()
+{
+    int d = current_device();
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    if (!g_sms[d]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+        g_sms[d] = v > 0 ? v : 1;
+    }
+    return g_sms[d];
+}
+
+// ---------------------------------------------------------------- per-thread context
+// One non-blocking stream per host thread and device for the host entry
+// points; device buffers come from the stream-ordered pool (cached between
+// calls, so repeated gateway calls do not pay cudaMalloc).
+struct HostCtx {
+    cudaStream_t stream[kMaxDevices] = {};
+};
+static thread_local HostCtx t_ctx;
+
+mela_status host_stream(cudaStream_t *s)
+{
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device visible");
+        return MELA_ERR_NO_DEVICE;
+    }
+    int d = current_device();
+    if (!t_ctx.stream[d]) {
+        MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.stream[d], cudaStreamNonBlocking));
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, d) == cudaSuccess) {
+            unsigned long long thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    *s = t_ctx.stream[d];
+    return MELA_OK;
+}
+
+DevBuf::~DevBuf()
+{
+    if (p) cudaFreeAsync(p, s);
+}
+
+mela_status DevBuf::alloc(size_t bytes, cudaStream_t st)
+{
+    s = st;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return cuda_status(e, "cudaMallocAsync");
+    }
+    return MELA_OK;
+}
+
+mela_status finish(cudaStream_t s)
+{
+    MELA_CUDA_TRY(cudaStreamSynchronize(s));
+    u32 flags = 0;
+    if (mela_device_error_flags(&flags, 1) == MELA_OK && (flags & kErrWaitTimeout)) {
+        set_error("a bounded device-side wait timed out");
+        return MELA_ERR_TIMEOUT;
+    }
+    return MELA_OK;
+}
+
+// ---------------------------------------------------------------- products
+i64 even_words(i64 bits)
+{
+    i64 w = words_of(bits);
+    return (w + 1) & ~1LL;
+}
+
+static i64 round_up(i64 x, i64 a) { return (x + a - 1) / a * a; }
+
+// workspace layout for each variant
+struct GemmPlan {
+    int variant;
+    i64 ldbt;             // packed Bt row pitch (words)
+    size_t bt_bytes;      // packed Bt
+    i64 mp, np, kp;       // padded byte-operand shape (tensor cores)
+    size_t a8_bytes, b8_bytes;
+    size_t total;
+};
+
+int choose_gemm_variant(i64 m, i64 k, i64 n)
+{
+    // Tensor cores pay off once every dimension spans a few tiles; below that
+    // the expansion to bytes dominates.  (The autotuner refines this table.)
+    if (m >= 1024 && n >= 1024 && k >= 1024) return MELA_GEMM_TC;
+    return MELA_GEMM_PLAIN;
+}
+
+static GemmPlan plan_gemm(int variant, i64 m, i64 k, i64 n)
+{
+    GemmPlan p{};
+    if (variant == MELA_GEMM_AUTO) variant = choose_gemm_variant(m, k, n);
+    p.variant = variant;
+    p.ldbt = even_words(k);
+    if (variant == MELA_GEMM_PLAIN || variant == MELA_GEMM_TC) p.bt_bytes = (size_t)n * p.ldbt * 8;
+    if (variant == MELA_GEMM_TC) {
+        p.mp = round_up(m, 128);
+        p.np = round_up(n, 256);
+        p.kp = round_up(k, 128);
+        p.a8_bytes = (size_t)p.mp * p.kp;
+        p.b8_bytes = (size_t)p.np * p.kp;
+    }
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    p.total = al(p.bt_bytes) + al(p.a8_bytes) + al(p.b8_bytes);
+    return p;
+}
+
+struct GemmBufs {
+    u64 *Bt;
+    unsigned char *A8, *B8;
+};
+
+static GemmBufs carve(const GemmPlan &p, void *ws)
+{
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    unsigned char *w = (unsigned char *)ws;
+    GemmBufs b;
+    b.Bt = (u64 *)w;
+    b.A8 = w + al(p.bt_bytes);
+    b.B8 = b.A8 + al(p.a8_bytes);
+    return b;
+}
+
+static mela_status check_ws(const GemmPlan &p, void *ws, size_t ws_bytes)
+{
+    if (ws_bytes < p.total || (p.total && !ws)) {
+        set_error("mela_dev_matmul: workspace of %zu bytes needed, %zu given", p.total, ws_bytes);
+        return MELA_ERR_INVALID;
+    }
+    return MELA_OK;
+}
+
+// Operand preparation: B transposed (plain and tensor-core forms) and the
+// 0/1 byte expansion of A and Bt (tensor-core form).
+mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, i64 m, i64 k,
+                         i64 n, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (m == 0 || n == 0 || k == 0) return MELA_OK;
+    GemmPlan p = plan_gemm(variant, m, k, n);
+    mela_status st = check_ws(p, ws, ws_bytes);
+    if (st != MELA_OK) return st;
+    GemmBufs b = carve(p, ws);
+    if (p.variant == MELA_GEMM_PLAIN || p.variant == MELA_GEMM_TC) {
+        if ((st = launch_transpose(B, ldb, k, n, b.Bt, p.ldbt, s)) != MELA_OK) return st;
+        if (p.ldbt > words_of(k)) {
+            // the pad word of each Bt row must read as zero
+            MELA_CUDA_TRY(cudaMemset2DAsync(b.Bt + words_of(k), (size_t)p.ldbt * 8, 0, 8, (size_t)n, s));
+        }
+    }
+    if (p.variant == MELA_GEMM_TC) {
+        if ((st = launch_expand_u8(A, lda, m, k, p.mp, p.kp, b.A8, s)) != MELA_OK) return st;
+        if ((st = launch_expand_u8(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)) != MELA_OK) return st;
+    }
+    return MELA_OK;
+}
+
+// The product kernel itself on prepared operands.
+mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
+                     i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (m == 0 || n == 0) return MELA_OK;
+    if (k == 0) {
+        MELA_CUDA_TRY(cudaMemset2DAsync(C, (size_t)ldc * 8, 0, (size_t)words_of(n) * 8, (size_t)m, s));
+        return MELA_OK;
+    }
+    GemmPlan p = plan_gemm(variant, m, k, n);
+    mela_status st = check_ws(p, ws, ws_bytes);
+    if (st != MELA_OK) return st;
+    GemmBufs b = carve(p, ws);
+    switch (p.variant) {
+    case MELA_GEMM_PLAIN: return launch_gemm_plain(A, lda, b.Bt, p.ldbt, C, ldc, m, k, n, s);
+    case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s);
+    case MELA_GEMM_M4RI: return launch_gemm_m4ri(A, lda, B, ldb, C, ldc, m, k, n, s);
+    default:
+        set_error("unknown product variant %d", p.variant);
+        return MELA_ERR_INVALID;
+    }
+}
+
+mela_status gemm_device(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
+                        i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    mela_status st = gemm_prepare(variant, A, lda, B, ldb, m, k, n, ws, ws_bytes, s);
+    if (st != MELA_OK) return st;
+    return gemm_run(variant, A, lda, B, ldb, C, ldc, m, k, n, ws, ws_bytes, s);
+}
+
+size_t gemm_workspace(int variant, i64 m, i64 k, i64 n)
+{
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    return plan_gemm(variant, m, k, n).total;
+}
+
+// ---------------------------------------------------------------- host-matrix helpers
+mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStream_t s,
+                            DevBuf &staging)
+{
+    const i64 m = M->rows, n = M->cols;
+    if (m == 0 || n == 0) {
+        if (m > 0) MELA_CUDA_TRY(cudaMemsetAsync(dP, 0, (size_t)m * ld * 8, s));
+        return MELA_OK;
+    }
+    const size_t esz = M->kind == MELA_KIND_DOUBLE ? 8 : 1;
+    const size_t bytes = (size_t)m * (size_t)n * esz;
+    mela_status st = staging.alloc(bytes, s);
+    if (st != MELA_OK) return st;
+    MELA_CUDA_TRY(cudaMemcpyAsync(staging.p, M->data, bytes, cudaMemcpyHostToDevice, s));
+    return launch_pack(M->kind, m, n, staging.p, dP, ld, s);
+}
+
+}  // namespace mela
+
+// ---------------------------------------------------------------- C ABI
+using namespace mela;
+
+extern "C" int mela_version(void) { return 10000; }
+
+extern "C" const char *mela_status_string(mela_status s)
+{
+    switch (s) {
+    case MELA_OK: return "ok";
+    case MELA_ERR_INVALID: return "invalid argument";
+    case MELA_ERR_SPARSE: return "sparse input not supported";
+    case MELA_ERR_DIM: return "inner dimensions must agree";
+    case MELA_ERR_TYPE: return "input must be logical or double";
+    case MELA_ERR_NOMEM: return "out of memory";
+    case MELA_ERR_CUDA: return "CUDA error";
+    case MELA_ERR_TIMEOUT: return "device wait timed out";
+    case MELA_ERR_UNSUPPORTED: return "unsupported";
+    case MELA_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char *mela_last_error(void) { return t_err; }
+
+extern "C" mela_status mela_device_error_flags(uint32_t *flags, int clear)
+{
+    u32 *p = device_error_word();
+    if (!p) {
+        set_error("device error word unavailable");
+        return MELA_ERR_CUDA;
+    }
+    u32 v = 0;
+    MELA_CUDA_TRY(cudaMemcpy(&v, p, 4, cudaMemcpyDeviceToHost));
+    if (clear && v) MELA_CUDA_TRY(cudaMemset(p, 0, 4));
+    if (flags) *flags = v;
+    return MELA_OK;
+}
+
+extern "C" size_t mela_matmul_workspace_size(int32_t variant, int64_t m, int64_t k, int64_t n)
+{
+    if (variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC) return 0;
+    return gemm_workspace(variant, m, k, n);
+}
+
+extern "C" mela_status mela_dev_matmul(int32_t variant, const uint64_t *dA, int64_t lda,
+                                       const uint64_t *dB, int64_t ldb, uint64_t *dC, int64_t ldc,
+                                       int64_t m, int64_t k, int64_t n, void *workspace,
+                                       size_t workspace_bytes, void *stream)
+{
+    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC ||
+        lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
+        set_error("mela_dev_matmul: bad shape, leading dimension or variant");
+        return MELA_ERR_INVALID;
+    }
+    if (m > 0 && n > 0 && (!dC || (k > 0 && (!dA || !dB)))) {
+        set_error("mela_dev_matmul: null operand");
+        return MELA_ERR_INVALID;
+    }
+    return gemm_device(variant, (const u64 *)dA, lda, (const u64 *)dB, ldb, (u64 *)dC, ldc, m, k,
+                       n, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+static mela_status check_dev_matmul_args(int32_t variant, const uint64_t *dA, int64_t lda,
+                                         const uint64_t *dB, int64_t ldb, int64_t ldc, int64_t m,
+                                         int64_t k, int64_t n)
+{
+    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC ||
+        lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
+        set_error("bad shape, leading dimension or variant");
+        return MELA_ERR_INVALID;
+    }
+    if (m > 0 && n > 0 && k > 0 && (!dA || !dB)) {
+        set_error("null operand");
+        return MELA_ERR_INVALID;
+    }
+    return MELA_OK;
+}
+
+extern "C" mela_status mela_dev_matmul_prepare(int32_t variant, const uint64_t *dA, int64_t lda,
+                                               const uint64_t *dB, int64_t ldb, int64_t m,
+                                               int64_t k, int64_t n, void *workspace,
+                                               size_t workspace_bytes, void *stream)
+{
+    mela_status st = check_dev_matmul_args(variant, dA, lda, dB, ldb, words_of(n), m, k, n);
+    if (st != MELA_OK) return st;
+    return gemm_prepare(variant, (const u64 *)dA, lda, (const u64 *)dB, ldb, m, k, n, workspace,
+                        workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, int64_t lda,
+                                           const uint64_t *dB, int64_t ldb, uint64_t *dC,
+                                           int64_t ldc, int64_t m, int64_t k, int64_t n,
+                                           void *workspace, size_t workspace_bytes, void *stream)
+{
+    mela_status st = check_dev_matmul_args(variant, dA, lda, dB, ldb, ldc, m, k, n);
+    if (st != MELA_OK) return st;
+    if (m > 0 && n > 0 && !dC) {
+        set_error("null output");
+        return MELA_ERR_INVALID;
+    }
+    return gemm_run(variant, (const u64 *)dA, lda, (const u64 *)dB, ldb, (u64 *)dC, ldc, m, k, n,
+                    workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, const uint64_t *B,
+                                               int64_t ldb, uint64_t *C, int64_t ldc, int64_t m,
+                                               int64_t k, int64_t n, int32_t variant)
+{
+    if (m < 0 || k < 0 || n < 0 || lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n) ||
+        variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC) {
+        set_error("mela_matmul_packed_host: bad shape or variant");
+        return MELA_ERR_INVALID;
+    }
+    if (m == 0 || n == 0) return MELA_OK;
+    cudaStream_t s;
+    mela_status st = host_stream(&s);
+    if (st != MELA_OK) return st;
+    const i64 wk = words_of(k), wn = words_of(n);
+    DevBuf dA, dB, dC, ws;
+    if ((st = dA.alloc((size_t)m * (wk ? wk : 1) * 8, s)) != MELA_OK) return st;
+    if ((st = dB.alloc((size_t)(k ? k : 1) * wn * 8, s)) != MELA_OK) return st;
+    if ((st = dC.alloc((size_t)m * wn * 8, s)) != MELA_OK) return st;
+    size_t wsb = gemm_workspace(variant, m, k, n);
+    if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
+    if (k > 0) {
+        MELA_CUDA_TRY(cudaMemcpy2DAsync(dA.p, (size_t)wk * 8, A, (size_t)lda * 8, (size_t)wk * 8,
+                                        (size_t)m, cudaMemcpyHostToDevice, s));
+        MELA_CUDA_TRY(cudaMemcpy2DAsync(dB.p, (size_t)wn * 8, B, (size_t)ldb * 8, (size_t)wn * 8,
+                                        (size_t)k, cudaMemcpyHostToDevice, s));
+    }
+    st = gemm_device(variant, (const u64 *)dA.p, wk, (const u64 *)dB.p, wn, (u64 *)dC.p, wn, m, k, n,
+                     ws.p, wsb, s);
+    if (st != MELA_OK) return st;
+    MELA_CUDA_TRY(cudaMemcpy2DAsync(C, (size_t)ldc * 8, dC.p, (size_t)wn * 8, (size_t)wn * 8,
+                                    (size_t)m, cudaMemcpyDeviceToHost, s));
+    return finish(s);
+}
+
+// Shared body of the two product gateways (reference validation order:
+// src/mela_matmul_gf2.c:75-88).
+static mela_status matmul_host(const mela_host_matrix *A, const mela_host_matrix *B, uint8_t *C,
+                               int variant)
+{
+    if (!A || !B) {
+        set_error("null argument");
+        return MELA_ERR_INVALID;
+    }
+    if (A->sparse || B->sparse) return MELA_ERR_SPARSE;
+    if (A->cols != B->rows) return MELA_ERR_DIM;
+    auto ok_kind = [](int k) { return k == MELA_KIND_LOGICAL || k == MELA_KIND_DOUBLE; };
+    if (!ok_kind(A->kind) || !ok_kind(B->kind)) return MELA_ERR_TYPE;
+    const i64 m = A->rows, k = A->cols, n = B->cols;
+    if (m < 0 || k < 0 || n < 0) return MELA_ERR_INVALID;
+    if (m == 0 || n == 0) return MELA_OK;
+    if (!C || (k > 0 && (!A->data || !B->data))) {
+        set_error("null data pointer");
+        return MELA_ERR_INVALID;
+    }
+    cudaStream_t s;
+    mela_status st = host_stream(&s);
+    if (st != MELA_OK) return st;
+    const i64 lda = even_words(k), ldb = even_words(n), ldc = even_words(n);
+    DevBuf pA, pB, pC, sA, sB, ws, outb;
+    if ((st = pA.alloc((size_t)m * lda * 8, s)) != MELA_OK) return st;
+    if ((st = pB.alloc((size_t)(k ? k : 1) * ldb * 8, s)) != MELA_OK) return st;
+    if ((st = pC.alloc((size_t)m * ldc * 8, s)) != MELA_OK) return st;
+    if ((st = upload_and_pack(A, (u64 *)pA.p, lda, s, sA)) != MELA_OK) return st;
+    if ((st = upload_and_pack(B, (u64 *)pB.p, ldb, s, sB)) != MELA_OK) return st;
+    size_t wsb = gemm_workspace(variant, m, k, n);
+    if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
+    st = gemm_device(variant, (const u64 *)pA.p, lda, (const u64 *)pB.p, ldb, (u64 *)pC.p, ldc, m,
+                     k, n, ws.p, wsb, s);
+    if (st != MELA_OK) return st;
+    if ((st = outb.alloc((size_t)m * n, s)) != MELA_OK) return st;
+    if ((st = launch_unpack((const u64 *)pC.p, ldc, m, n, (unsigned char *)outb.p, s)) != MELA_OK)
+        return st;
+    MELA_CUDA_TRY(cudaMemcpyAsync(C, outb.p, (size_t)m * n, cudaMemcpyDeviceToHost, s));
+    return finish(s);
+}
+
+extern "C" mela_status mela_matmul_gf2(const mela_host_matrix *A, const mela_host_matrix *B,
+                                       uint8_t *C)
+{
+    return matmul_host(A, B, C, MELA_GEMM_AUTO);
+}
+
+extern "C" mela_status mela_matmul_m4ri(const mela_host_matrix *A, const mela_host_matrix *B,
+                                        uint8_t *C)
+{
+    return matmul_host(A, B, C, MELA_GEMM_M4RI);
+}

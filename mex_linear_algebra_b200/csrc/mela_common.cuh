@@ -1,0 +1,62 @@
+// mela_common.cuh -- shared device/host helpers of the sm_100a GF(2) library.
+//
+// Packed layout used by every kernel: row-major uint64 words, bit j of row i
+// in word i*ld + (j >> 6) at bit position (j & 63) -- the reference library's
+// own convention (src/mela_matmul_gf2.c:33-36).  Bits at columns >= n of the
+// last word of a row are zero on every packed buffer this library writes.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "../../include/mela.h"
+
+namespace mela {
+
+using u64 = unsigned long long;
+using u32 = unsigned int;
+using i64 = long long;
+
+constexpr int kWordBits = 64;
+__host__ __device__ inline i64 words_of(i64 n) { return (n + 63) >> 6; }
+
+// ---------------------------------------------------------------- errors
+// Thread-local detail message of the last failure (host side).
+void set_error(const char *fmt, ...);
+mela_status cuda_status(cudaError_t e, const char *what);
+
+#define MELA_CUDA_TRY(expr)                                        \
+    do {                                                           \
+        cudaError_t _e = (expr);                                   \
+        if (_e != cudaSuccess) return ::mela::cuda_status(_e, #expr); \
+    } while (0)
+
+#define MELA_LAUNCH_CHECK(what)                                    \
+    do {                                                           \
+        cudaError_t _e = cudaGetLastError();                       \
+        if (_e != cudaSuccess) return ::mela::cuda_status(_e, what); \
+    } while (0)
+
+// Device-side error word.  Kernels whose waits can run out set a bit here
+// instead of trapping; the host reads it with mela_device_error_flags().
+enum : u32 {
+    kErrWaitTimeout = 1u << 0,   // an mbarrier / flag wait ran past its limit
+    kErrBadArgument = 1u << 1,   // a kernel-side bounds check rejected its input
+};
+u32 *device_error_word();  // per-device __device__ word (address on current device)
+
+// Timeout for every bounded device-side wait: about two seconds.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------- launch sizing
+int sm_count();  // multiprocessors of the current device (cached per device)
+
+}  // namespace mela

@@ -1,0 +1,41 @@
+// mela_host.h -- host-layer helpers shared by the C-ABI translation units.
+#pragma once
+
+#include "mela_common.cuh"
+
+namespace mela {
+
+// Stream-ordered device buffer from the default memory pool, released on
+// the same stream when it goes out of scope.
+struct DevBuf {
+    void *p = nullptr;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf();
+    mela_status alloc(size_t bytes, cudaStream_t st);
+};
+
+// The calling thread's library stream on the current device.
+mela_status host_stream(cudaStream_t *s);
+// Synchronise `s` and turn a device-side wait timeout into MELA_ERR_TIMEOUT.
+mela_status finish(cudaStream_t s);
+
+// Row pitch in words, rounded up to an even count (16-byte rows).
+i64 even_words(i64 bits);
+
+int choose_gemm_variant(i64 m, i64 k, i64 n);
+size_t gemm_workspace(int variant, i64 m, i64 k, i64 n);
+mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, i64 m, i64 k,
+                         i64 n, void *ws, size_t ws_bytes, cudaStream_t s);
+mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
+                     i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s);
+mela_status gemm_device(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
+                        i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s);
+
+// Copy a host MATLAB array to the device and pack it into dP (ld words/row).
+mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStream_t s,
+                            DevBuf &staging);
+
+}  // namespace mela

@@ -1,0 +1,283 @@
+// pack.cu -- data-format kernels on the path into and out of the GF(2) kernels.
+//
+//  * rand_dense   seeded Bernoulli(1/2) packed matrices (counter-based
+//                 splitmix64, identical bits to the CPU generator)
+//  * pack         MATLAB column-major logical / double -> packed rows
+//                 (reference: pack_rows_logical / pack_rows_double,
+//                 src/mela_matmul_gf2.c:42-69; inline packs in
+//                 src/mela_rank_gf2.c:154-176, src/mela_null_gf2.c:169-187)
+//  * unpack       packed rows -> column-major logical bytes
+//                 (reference: src/mela_matmul_gf2.c:193-205)
+//  * transpose    64x64 bit-block transpose with warp ballots
+//  * expand_u8    packed bits -> 0/1 bytes (operands of the tensor-core GEMM)
+//
+// All of these are HBM-bound byte/word moves: each thread reads and writes
+// whole words or bytes with warp-contiguous addresses; no GEMM reshaping.
+#include "mela_common.cuh"
+#include "mela_internal.h"
+
+namespace mela {
+
+// ---------------------------------------------------------------- generator
+__host__ __device__ __forceinline__ u64 mix64(u64 z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+u64 stream_key(u64 seed, u64 stream)
+{
+    return mix64(seed * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL) ^
+           mix64(stream + 0xD1B54A32D192ED03ULL);
+}
+
+__global__ void rand_dense_kernel(u64 key, i64 m, i64 n, i64 wc, u64 *out, i64 ld)
+{
+    const u64 tail = (n & 63) ? ((1ULL << (n & 63)) - 1) : ~0ULL;
+    i64 total = m * ld;
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total;
+         t += (i64)gridDim.x * blockDim.x) {
+        i64 i = t / ld, w = t - i * ld;
+        u64 v = 0;
+        if (w < wc) {
+            v = mix64(key + (u64)(i * wc + w + 1) * 0x9E3779B97F4A7C15ULL);
+            if (w == wc - 1) v &= tail;
+        }
+        out[t] = v;
+    }
+}
+
+// ---------------------------------------------------------------- pack
+// Parity of a double as the reference reads it, ((int)x) & 1, with the
+// x86-64 result for NaN and out-of-range values (INT_MIN, even) spelled out.
+__device__ __forceinline__ u32 parity_of(double x)
+{
+    if (!(x >= -2147483648.0 && x < 2147483648.0)) return 0;
+    return (u32)__double2int_rz(x) & 1u;
+}
+__device__ __forceinline__ u32 parity_of(unsigned char x) { return x != 0; }
+
+// One block: 32 rows x 8 output words (512 columns).  Warp w builds word
+// column w: lane l owns row row0+l and walks the 64 columns of its word,
+// so each load instruction reads 32 consecutive rows of one column.
+template <typename T>
+__global__ void __launch_bounds__(256) pack_kernel(const T *__restrict__ in, i64 m, i64 n,
+                                                   u64 *__restrict__ out, i64 ld)
+{
+    __shared__ u64 tile[32][9];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const i64 row0 = (i64)blockIdx.x * 32;
+    const i64 w = (i64)blockIdx.y * 8 + warp;
+    const i64 row = row0 + lane;
+    u64 word = 0;
+    if (row < m && w * 64 < n) {
+        const i64 c0 = w * 64;
+        const int cols = (int)((n - c0) < 64 ? (n - c0) : 64);
+        const T *p = in + row + c0 * m;
+        for (int j = 0; j < cols; ++j) word |= (u64)parity_of(p[(i64)j * m]) << j;
+    }
+    tile[lane][warp] = word;
+    __syncthreads();
+    const int r = threadIdx.x >> 3, q = threadIdx.x & 7;
+    const i64 orow = row0 + r, ow = (i64)blockIdx.y * 8 + q;
+    if (orow < m && ow < ld) out[orow * ld + ow] = tile[r][q];
+}
+
+// ---------------------------------------------------------------- unpack
+// One warp: 32 rows x 64 columns; each store instruction writes 32
+// consecutive rows of one column (column-major output).
+__global__ void __launch_bounds__(256) unpack_kernel(const u64 *__restrict__ in, i64 ld, i64 m,
+                                                     i64 n, unsigned char *__restrict__ out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const i64 row = (i64)blockIdx.x * 32 + lane;
+    const i64 w = (i64)blockIdx.y * 8 + warp;
+    if (w * 64 >= n) return;
+    const i64 c0 = w * 64;
+    const int cols = (int)((n - c0) < 64 ? (n - c0) : 64);
+    if (row >= m) return;
+    u64 word = in[row * ld + w];
+    unsigned char *p = out + row + c0 * m;
+    for (int j = 0; j < cols; ++j) p[(i64)j * m] = (unsigned char)((word >> j) & 1);
+}
+
+// ---------------------------------------------------------------- transpose
+// Block: 256 input rows x 64 input columns.  Warp w loads rows
+// 32w..32w+31 (one word each); 64 ballots give, per input column b, the 32
+// bits of rows 32w..32w+31.  Output row (column b) receives 4 words.
+__global__ void __launch_bounds__(256) transpose_kernel(const u64 *__restrict__ in, i64 ld_in,
+                                                        i64 rows, i64 cols,
+                                                        u64 *__restrict__ out, i64 ld_out)
+{
+    __shared__ u32 part[8][65];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const i64 wcol = blockIdx.x;           // input word column
+    const i64 r0 = (i64)blockIdx.y * 256;  // input row group
+    const i64 row = r0 + warp * 32 + lane;
+    u64 x = (row < rows) ? in[row * ld_in + wcol] : 0ull;
+    u32 keep0 = 0, keep1 = 0;
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {
+        u32 v = __ballot_sync(0xffffffffu, (u32)(x >> b) & 1u);
+        if (lane == b) keep0 = v;
+    }
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {
+        u32 v = __ballot_sync(0xffffffffu, (u32)(x >> (b + 32)) & 1u);
+        if (lane == b) keep1 = v;
+    }
+    part[warp][lane] = keep0;
+    part[warp][lane + 32] = keep1;
+    __syncthreads();
+    const int b = threadIdx.x >> 2, q = threadIdx.x & 3;
+    const i64 ocol_row = wcol * 64 + b;  // output row index
+    const i64 ow = (i64)blockIdx.y * 4 + q;
+    const i64 owc = words_of(rows);
+    if (ocol_row < cols && ow < owc)
+        out[ocol_row * ld_out + ow] = (u64)part[2 * q][b] | ((u64)part[2 * q + 1][b] << 32);
+}
+
+// ---------------------------------------------------------------- expand to bytes
+// out[r][k] = bit k of packed row r, for r < rows_pad, k < kpad (multiple of
+// 64); zero outside rows x kbits.  One thread per 64-bit word -> 64 bytes.
+__device__ __forceinline__ u32 spread4(u32 nib) { return (nib * 0x00204081u) & 0x01010101u; }
+
+__global__ void __launch_bounds__(256) expand_u8_kernel(const u64 *__restrict__ in, i64 ld,
+                                                        i64 rows, i64 kbits, i64 rows_pad,
+                                                        i64 kpad, unsigned char *__restrict__ out)
+{
+    const i64 wpr = kpad >> 6;  // words per padded row
+    const i64 total = rows_pad * wpr;
+    const i64 wc = words_of(kbits);
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total;
+         t += (i64)gridDim.x * blockDim.x) {
+        const i64 r = t / wpr, w = t - r * wpr;
+        u64 v = (r < rows && w < wc) ? in[r * ld + w] : 0ull;
+        uint4 *dst = reinterpret_cast<uint4 *>(out + r * kpad + w * 64);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            u32 h = (u32)(v >> (16 * q));
+            uint4 o;
+            o.x = spread4(h & 15);
+            o.y = spread4((h >> 4) & 15);
+            o.z = spread4((h >> 8) & 15);
+            o.w = spread4((h >> 12) & 15);
+            dst[q] = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static int grid_for(i64 total, int threads)
+{
+    i64 g = (total + threads - 1) / threads;
+    i64 cap = (i64)sm_count() * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+mela_status launch_expand_u8(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad,
+                             unsigned char *out, cudaStream_t s)
+{
+    i64 total = rows_pad * (kpad >> 6);
+    expand_u8_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, ld, rows, kbits, rows_pad, kpad, out);
+    MELA_LAUNCH_CHECK("expand_u8_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *out, i64 ld_out,
+                             cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0) return MELA_OK;
+    dim3 grid((unsigned)words_of(cols), (unsigned)((rows + 255) / 256));
+    transpose_kernel<<<grid, 256, 0, s>>>(in, ld_in, rows, cols, out, ld_out);
+    MELA_LAUNCH_CHECK("transpose_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, cudaStream_t s)
+{
+    if (m <= 0) return MELA_OK;
+    i64 wgroups = (ld + 7) / 8;
+    if (wgroups == 0) return MELA_OK;
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)wgroups);
+    if (kind == MELA_KIND_DOUBLE)
+        pack_kernel<double><<<grid, 256, 0, s>>>((const double *)in, m, n, out, ld);
+    else
+        pack_kernel<unsigned char><<<grid, 256, 0, s>>>((const unsigned char *)in, m, n, out, ld);
+    MELA_LAUNCH_CHECK("pack_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *out, cudaStream_t s)
+{
+    if (m <= 0 || n <= 0) return MELA_OK;
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((words_of(n) + 7) / 8));
+    unpack_kernel<<<grid, 256, 0, s>>>(in, ld, m, n, out);
+    MELA_LAUNCH_CHECK("unpack_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_rand_dense(u64 seed, u64 stream_id, i64 m, i64 n, u64 *out, i64 ld,
+                              cudaStream_t s)
+{
+    if (m <= 0 || ld <= 0) return MELA_OK;
+    rand_dense_kernel<<<grid_for(m * ld, 256), 256, 0, s>>>(stream_key(seed, stream_id), m, n,
+                                                            words_of(n), out, ld);
+    MELA_LAUNCH_CHECK("rand_dense_kernel");
+    return MELA_OK;
+}
+
+}  // namespace mela
+
+// ---------------------------------------------------------------- C ABI
+using namespace mela;
+
+extern "C" mela_status mela_dev_rand_dense(uint64_t seed, uint64_t stream_id, int64_t m,
+                                           int64_t n, uint64_t *d_out, int64_t ld, void *stream)
+{
+    if (m < 0 || n < 0 || ld < words_of(n) || (m > 0 && ld > 0 && !d_out)) {
+        set_error("mela_dev_rand_dense: bad shape or pointer");
+        return MELA_ERR_INVALID;
+    }
+    return launch_rand_dense(seed, stream_id, m, n, (u64 *)d_out, ld, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_dev_pack(int32_t kind, int64_t m, int64_t n, const void *d_in,
+                                     uint64_t *d_out, int64_t ld, void *stream)
+{
+    if (m < 0 || n < 0 || ld < words_of(n) || (kind != MELA_KIND_LOGICAL && kind != MELA_KIND_DOUBLE)) {
+        set_error("mela_dev_pack: bad shape or kind");
+        return MELA_ERR_INVALID;
+    }
+    if (m > 0 && ld > 0 && (!d_out || (n > 0 && !d_in))) {
+        set_error("mela_dev_pack: null pointer");
+        return MELA_ERR_INVALID;
+    }
+    return launch_pack(kind, m, n, d_in, (u64 *)d_out, ld, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_dev_unpack(const uint64_t *d_in, int64_t ld, int64_t m, int64_t n,
+                                       uint8_t *d_out, void *stream)
+{
+    if (m < 0 || n < 0 || ld < words_of(n) || (m > 0 && n > 0 && (!d_in || !d_out))) {
+        set_error("mela_dev_unpack: bad shape or pointer");
+        return MELA_ERR_INVALID;
+    }
+    return launch_unpack((const u64 *)d_in, ld, m, n, d_out, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_dev_transpose(const uint64_t *d_in, int64_t ld_in, int64_t rows,
+                                          int64_t cols, uint64_t *d_out, int64_t ld_out,
+                                          void *stream)
+{
+    if (rows < 0 || cols < 0 || ld_in < words_of(cols) || ld_out < words_of(rows) ||
+        (rows > 0 && cols > 0 && (!d_in || !d_out))) {
+        set_error("mela_dev_transpose: bad shape or pointer");
+        return MELA_ERR_INVALID;
+    }
+    return launch_transpose((const u64 *)d_in, ld_in, rows, cols, (u64 *)d_out, ld_out,
+                            (cudaStream_t)stream);
+}
