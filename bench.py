@@ -39,6 +39,12 @@ sys.path.insert(0, ROOT)
 M = K = N = 32768
 SEED = 1
 BITOPS = 2.0 * M * N * K
+
+
+def set_size(size: int) -> None:
+    global M, K, N, BITOPS
+    M = K = N = size
+    BITOPS = 2.0 * M * N * K
 CPU_SAMPLE = (2048, 32768, 2048)  # rows of A, K, columns of B for the CPU legs
 
 
@@ -276,6 +282,35 @@ def run_mela(args, ws, rank, local):
         ok = bool(torch.equal(Cp, C[:rows]))
     flags = D.device_error_flags()
 
+    # the same product through the CUDA-core forms (one timed call each)
+    forms = {"tc_ms": round(ms_step, 3)}
+    if not args.quick:
+        for name, var in (("plain", _lib.GEMM_PLAIN), ("m4ri", _lib.GEMM_M4RI)):
+            wsv = D.matmul_workspace(var, M, K, N)
+            wv = torch.empty(max(wsv, 1), dtype=torch.uint8, device="cuda")
+            Cv = torch.empty_like(C)
+            def run_form():
+                check(L.mela_dev_matmul(var, A.data_ptr(), wk, B.data_ptr(), wn, Cv.data_ptr(), wn,
+                                        M, K, N, wv.data_ptr(), wsv, sptr))
+            run_form()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run_form()
+            e1.record(stream)
+            e1.synchronize()
+            forms[name + "_ms"] = round(e0.elapsed_time(e1), 3)
+            forms[name + "_equal"] = bool(torch.equal(Cv, C))
+            del wv, Cv
+        forms["tc_over_plain"] = round(forms["plain_ms"] / ms_step, 2)
+        forms["tc_over_m4ri"] = round(forms["m4ri_ms"] / ms_step, 2)
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": "GF(2) GEMM Tbitop/s", "value": round(value, 3),
+                              "unit": "Tbitop/s", "ms_per_step": round(ms_step, 4),
+                              "kernel_ms": round(kern_avg, 4), "size": M, "result_check": ok}))
+        return 0 if ok else 1
+
     # e2e through the C ABI with pinned host buffers
     e2e = None
     del work
@@ -346,6 +381,7 @@ def run_mela(args, ws, rank, local):
                                        f"{ks_}x{ns_}, one call"},
             "e2e": e2e,
             "gpu_launches": 4 * args.steps,
+            "forms": forms,
             "clocks": clk,
             "device_error_flags": flags,
         }
@@ -363,7 +399,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mela", "reference"], default="mela")
+    ap.add_argument("--size", type=int, default=32768,
+                    help="square problem size (32768 is the benchmark; smaller sizes are for profiling)")
+    ap.add_argument("--quick", action="store_true",
+                    help="device timing only: no e2e, CPU baseline, peak or form comparison")
     args = ap.parse_args()
+    set_size(args.size)
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
