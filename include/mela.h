@@ -148,6 +148,25 @@ mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, int64_t lda
                                 int64_t m, int64_t k, int64_t n, void *workspace,
                                 size_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* allocation-free product                                              */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference library.  For callers that are given
+ * device buffers but may not allocate device memory themselves (a plugin
+ * whose host application owns the GPU memory budget, or a latency-critical
+ * loop that cannot take cudaMalloc's implicit synchronisation): the plain
+ * AND+popcount product C = A*B with its one scratch buffer (B transposed)
+ * held in a fixed 16 MiB array inside the library instead of a caller
+ * workspace.  Limit: n * (ceil(k/64) rounded up to even) * 8 bytes must not
+ * exceed mela_static_scratch_bytes(); larger products return
+ * MELA_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race, so serialise them. */
+size_t mela_static_scratch_bytes(void);
+mela_status mela_dev_matmul_plain_static(const uint64_t *dA, int64_t lda, const uint64_t *dB,
+                                         int64_t ldb, uint64_t *dC, int64_t ldc, int64_t m,
+                                         int64_t k, int64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

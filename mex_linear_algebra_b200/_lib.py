@@ -45,6 +45,8 @@ SIGNATURES = {
     "mela_dev_matmul": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "mela_dev_matmul_prepare": (_st, [_i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "mela_dev_matmul_run": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "mela_static_scratch_bytes": (_sz, []),
+    "mela_dev_matmul_plain_static": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp]),
 }
 
 _lib = None
