@@ -72,6 +72,13 @@ typedef enum {
     MELA_GEMM_TC = 3      /* tcgen05 kind::i8 tensor cores, parity of the s32 sum */
 } mela_gemm_variant;
 
+/* Elimination variants (rank / RREF / null space); results are identical. */
+typedef enum {
+    MELA_ELIM_AUTO = 0,
+    MELA_ELIM_PLAIN = 1,  /* per-pivot warp-ballot search + broadcast-XOR sweep */
+    MELA_ELIM_M4RI = 2    /* 64-column panels, Gray-code tables in shared memory */
+} mela_elim_variant;
+
 /* ------------------------------------------------------------------ */
 /* library                                                             */
 /* ------------------------------------------------------------------ */
@@ -95,6 +102,53 @@ mela_status mela_matmul_gf2(const mela_host_matrix *A, const mela_host_matrix *B
 /* Same result through the Four-Russians kernel (src/mela_matmul_m4ri.c). */
 mela_status mela_matmul_m4ri(const mela_host_matrix *A, const mela_host_matrix *B,
                              uint8_t *C);
+
+/* Output allocator for the null-space entry points: returns a buffer of
+ * rows*cols bytes for the rows x cols logical result (column-major), or NULL
+ * when rows*cols is 0.  Called once, after the rank is known. */
+typedef uint8_t *(*mela_alloc_fn)(void *ctx, int64_t rows, int64_t cols);
+
+/* Rank over GF(2) (forward elimination, src/mela_rank_gf2.c:27-121 and
+ * src/mela_rank_m4ri.c:94-279).  Empty inputs have rank 0. */
+mela_status mela_rank_gf2(const mela_host_matrix *A, double *rank);
+mela_status mela_rank_m4ri(const mela_host_matrix *A, double *rank);
+
+/* Null-space basis Z (n x nullity logical, column-major): free columns f_i
+ * ascending, Z(f_i, i) = 1, Z(pivot column p, i) = RREF(p, f_i) -- the basis
+ * of src/mela_null_gf2.c:189-274 and src/mela_null_m4ri.c:298-401, bit for
+ * bit.  Sparse input -> MELA_ERR_SPARSE, other classes -> MELA_ERR_TYPE.
+ * m = 0 gives the identity (nullity n); n = 0 gives an empty result. */
+mela_status mela_null_gf2(const mela_host_matrix *H, mela_alloc_fn alloc, void *ctx,
+                          int64_t *nullity);
+mela_status mela_null_m4ri(const mela_host_matrix *H, mela_alloc_fn alloc, void *ctx,
+                           int64_t *nullity);
+
+/* ------------------------------------------------------------------ */
+/* gateway semantics (shared by the MEX files and other front ends)     */
+/* ------------------------------------------------------------------ */
+typedef enum {
+    MELA_FN_MATMUL_GF2 = 0,
+    MELA_FN_MATMUL_M4RI = 1,
+    MELA_FN_RANK_GF2 = 2,
+    MELA_FN_RANK_M4RI = 3,
+    MELA_FN_NULL_GF2 = 4,
+    MELA_FN_NULL_M4RI = 5
+} mela_function;
+
+/* Creates output `index` (kind MELA_KIND_LOGICAL or MELA_KIND_DOUBLE,
+ * rows x cols, column-major) and returns its data pointer. */
+typedef void *(*mela_gateway_alloc_fn)(void *ctx, int32_t index, int32_t kind, int64_t rows,
+                                       int64_t cols);
+typedef struct {
+    char id[64];   /* MATLAB error identifier ("" when the reference uses none) */
+    char msg[256]; /* error message text */
+} mela_gateway_error;
+
+/* Runs one reference gateway (mexFunction of src/mela_*.c) on host arrays:
+ * same argument checks in the same order, same error identifiers and
+ * messages, same outputs.  Returns 0 on success, 1 with *err filled. */
+int mela_gateway(int32_t fn, int32_t nlhs, int32_t nrhs, const mela_host_matrix *prhs,
+                 mela_gateway_alloc_fn alloc, void *ctx, mela_gateway_error *err);
 
 /* Host-resident packed product (copies in, computes, copies out). */
 mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, const uint64_t *B,
@@ -147,6 +201,33 @@ mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, int64_t lda
                                 const uint64_t *dB, int64_t ldb, uint64_t *dC, int64_t ldc,
                                 int64_t m, int64_t k, int64_t n, void *workspace,
                                 size_t workspace_bytes, void *stream);
+
+/* Workspace for mela_dev_rank / mela_dev_rref on an m x n matrix. */
+size_t mela_elim_workspace_size(int64_t m, int64_t n);
+/* Rank of the packed m x n matrix dM (overwritten).  Writes the rank to
+ * d_rank (device int64), the pivot columns to d_pivcols and the physical row
+ * holding each pivot row to d_pivrows (min(m, n) entries each). */
+mela_status mela_dev_rank(int32_t variant, uint64_t *dM, int64_t ld, int64_t m, int64_t n,
+                          int64_t *d_rank, int64_t *d_pivcols, int64_t *d_pivrows,
+                          void *workspace, size_t workspace_bytes, void *stream);
+/* Reduced row echelon form in place (gf2_rref_standard,
+ * src/mela_null_gf2.c:88-131): RREF row t is row d_pivrows[t] of dM, with
+ * its leading one in column d_pivcols[t] (ascending); rows that are not
+ * pivot rows end up zero. */
+mela_status mela_dev_rref(int32_t variant, uint64_t *dM, int64_t ld, int64_t m, int64_t n,
+                          int64_t *d_rank, int64_t *d_pivcols, int64_t *d_pivrows,
+                          void *workspace, size_t workspace_bytes, void *stream);
+size_t mela_null_workspace_size(int64_t n, int64_t rank);
+/* Null-space basis from an RREF (mela_dev_rref's outputs; `rank` on the
+ * host): Zt (n - rank rows of ldz words), row i = basis vector i, i.e.
+ * column i of the reference's n x nullity logical output. */
+mela_status mela_dev_null_basis(const uint64_t *dR, int64_t ld, int64_t m, int64_t n,
+                                int64_t rank, const int64_t *d_pivcols, const int64_t *d_pivrows,
+                                uint64_t *dZt, int64_t ldz, void *workspace,
+                                size_t workspace_bytes, void *stream);
+/* Packed rows -> row-major bytes (rows x n). */
+mela_status mela_dev_unpack_rows(const uint64_t *d_in, int64_t ld, int64_t rows, int64_t n,
+                                 uint8_t *d_out, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* allocation-free product                                              */

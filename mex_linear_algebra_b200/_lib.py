@@ -21,6 +21,21 @@ GEMM_AUTO, GEMM_PLAIN, GEMM_M4RI, GEMM_TC = 0, 1, 2, 3
 GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc": GEMM_TC}
 
 
+# mela_function (gateway ids)
+FN_MATMUL_GF2, FN_MATMUL_M4RI, FN_RANK_GF2, FN_RANK_M4RI, FN_NULL_GF2, FN_NULL_M4RI = range(6)
+# mela_elim_variant
+ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI = 0, 1, 2
+ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI}
+
+
+class GatewayError(C.Structure):
+    _fields_ = [("id", C.c_char * 64), ("msg", C.c_char * 256)]
+
+
+ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int64, C.c_int64)
+GATEWAY_ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64)
+
+
 class HostMatrix(C.Structure):
     _fields_ = [("kind", C.c_int32), ("sparse", C.c_int32), ("rows", C.c_int64),
                 ("cols", C.c_int64), ("data", C.c_void_p)]
@@ -36,6 +51,12 @@ SIGNATURES = {
     "mela_device_error_flags": (_st, [C.POINTER(_u32), C.c_int]),
     "mela_matmul_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
     "mela_matmul_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
+    "mela_rank_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(C.c_double)]),
+    "mela_rank_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(C.c_double)]),
+    "mela_null_gf2": (_st, [C.POINTER(HostMatrix), ALLOC_FN, _vp, C.POINTER(_i64)]),
+    "mela_null_m4ri": (_st, [C.POINTER(HostMatrix), ALLOC_FN, _vp, C.POINTER(_i64)]),
+    "mela_gateway": (C.c_int, [_i32, _i32, _i32, C.POINTER(HostMatrix), GATEWAY_ALLOC_FN, _vp,
+                               C.POINTER(GatewayError)]),
     "mela_matmul_packed_host": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i32]),
     "mela_dev_rand_dense": (_st, [_u64, _u64, _i64, _i64, _vp, _i64, _vp]),
     "mela_dev_pack": (_st, [_i32, _i64, _i64, _vp, _vp, _i64, _vp]),
@@ -45,6 +66,12 @@ SIGNATURES = {
     "mela_dev_matmul": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "mela_dev_matmul_prepare": (_st, [_i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "mela_dev_matmul_run": (_st, [_i32, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "mela_elim_workspace_size": (_sz, [_i64, _i64]),
+    "mela_dev_rank": (_st, [_i32, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "mela_dev_rref": (_st, [_i32, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "mela_null_workspace_size": (_sz, [_i64, _i64]),
+    "mela_dev_null_basis": (_st, [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _sz, _vp]),
+    "mela_dev_unpack_rows": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
     "mela_static_scratch_bytes": (_sz, []),
     "mela_dev_matmul_plain_static": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp]),
 }

@@ -46,6 +46,8 @@ typedef enum {
 /* Concrete layout of the host's arrays.  `data` is column-major, m*n
  * elements of the class's size.  `sparse` only flags the array (the host
  * keeps full storage): the gateways only ever ask mxIsSparse. */
+typedef enum { mxREAL = 0, mxCOMPLEX = 1 } mxComplexity;
+
 typedef struct mxArray_tag {
     mxClassID classid;
     mwSize m, n;
@@ -66,7 +68,7 @@ mxClassID mxGetClassID(const mxArray *a);
 
 mxArray *mxCreateLogicalMatrix(mwSize m, mwSize n);
 mxArray *mxCreateDoubleScalar(double v);
-mxArray *mxCreateDoubleMatrixReal(mwSize m, mwSize n);
+mxArray *mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity c);
 void mxDestroyArray(mxArray *a);
 
 void *mxCalloc(size_t n, size_t size);

@@ -131,7 +131,11 @@ static mxArray *create(mxClassID cls, mwSize m, mwSize n)
 
 mxArray *mxCreateLogicalMatrix(mwSize m, mwSize n) { return create(mxLOGICAL_CLASS, m, n); }
 
-mxArray *mxCreateDoubleMatrixReal(mwSize m, mwSize n) { return create(mxDOUBLE_CLASS, m, n); }
+mxArray *mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity c)
+{
+    (void)c; /* real storage only: the gateways create real outputs */
+    return create(mxDOUBLE_CLASS, m, n);
+}
 
 mxArray *mxCreateDoubleScalar(double v)
 {
