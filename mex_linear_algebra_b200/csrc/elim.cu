@@ -170,7 +170,10 @@ panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned ch
             rowk[h] = sm.R[0][b];
         }
     }
-    // Gauss-Jordan over the pivot bits, increasing
+    // Gauss-Jordan over the pivot bits, increasing.  The row chosen at step t
+    // keeps being reduced by later steps, so its combination is final only
+    // after the loop.
+    int step[2] = {-1, -1};
     u64 rest = pm;
     for (int t = 0; t < p; ++t) {
         const int b = ctz64(rest);
@@ -182,7 +185,6 @@ panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned ch
         const int sh = c0 ? 0 : 1;
         const u64 qs = __shfl_sync(0xffffffffu, sh ? q[1] : q[0], src);
         const u64 as = __shfl_sync(0xffffffffu, sh ? a[1] : a[0], src);
-        const int rs = __shfl_sync(0xffffffffu, sh ? rowk[1] : rowk[0], src);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const bool me = (lane == src && h == sh);
@@ -190,21 +192,25 @@ panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned ch
                 q[h] ^= qs;
                 a[h] ^= as;
             }
-            if (me) used[h] = true;
+            if (me) {
+                used[h] = true;
+                step[h] = t;
+            }
         }
-        if (lane == 0) {
-            ps->coef[t] = as;
-            ps->srow[t] = rs;
-            piv[r0 + t] = 64 * w + b;
-            prow[r0 + t] = rs;
-            state[rs] = 0;
-            stamp[rs] = panel;
-        }
+        if (lane == 0) piv[r0 + t] = 64 * w + b;
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int k = lane + 32 * h;
-        if (k < p) ps->sel[k] = rowk[h];
+        if (k < p) {
+            const int t = step[h];
+            ps->sel[k] = rowk[h];
+            ps->coef[t] = a[h];
+            ps->srow[t] = rowk[h];
+            prow[r0 + t] = rowk[h];
+            state[rowk[h]] = 0;
+            stamp[rowk[h]] = panel;
+        }
     }
     if (lane == 0) {
         ps->p = p;
