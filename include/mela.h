@@ -230,6 +230,39 @@ mela_status mela_dev_unpack_rows(const uint64_t *d_in, int64_t ld, int64_t rows,
                                  uint8_t *d_out, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* batched rank + null space                                            */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference (which handles one matrix per call).
+ * Many matrices of uneven shape are ranked and null-spaced in one
+ * persistent launch (replayed as a CUDA graph): a warp per small matrix, a
+ * 128-thread group per medium one, a whole CTA per large one.  Item i is
+ * packed at word offset in_offset of the input buffer (m rows of
+ * ceil(n/64) words; for the logical entry point: an m x n column-major
+ * logical array at byte offset sum_{j<i} m_j*n_j); its null-space basis is
+ * written at word offset z_offset of the output buffer as n - rank rows of
+ * ceil(n/64) words (room for n rows must be reserved), its rank to
+ * d_ranks[i].  Results equal mela_rank_gf2 / mela_null_gf2 per matrix. */
+typedef struct {
+    int64_t m, n;
+    int64_t in_offset; /* words */
+    int64_t z_offset;  /* words */
+} mela_batch_item;
+typedef struct mela_batch_plan mela_batch_plan;
+
+/* force_class: -1 = size-based (normal); 0/1/2 = run every item that fits
+ * with the CTA / 128-thread / warp engine (for testing the engines). */
+mela_status mela_batch_plan_create(const mela_batch_item *items, int64_t count,
+                                   int32_t force_class, mela_batch_plan **plan);
+void mela_batch_plan_destroy(mela_batch_plan *plan);
+mela_status mela_batch_plan_stats(const mela_batch_plan *plan, int64_t *big, int64_t *mid,
+                                  int64_t *small);
+mela_status mela_batch_rank_null(mela_batch_plan *plan, const uint64_t *d_in, uint64_t *d_zt,
+                                 int64_t *d_ranks, int32_t use_graph, void *stream);
+mela_status mela_batch_rank_null_logical(mela_batch_plan *plan, const uint8_t *d_in,
+                                         uint64_t *d_zt, int64_t *d_ranks, int32_t use_graph,
+                                         void *stream);
+
+/* ------------------------------------------------------------------ */
 /* allocation-free product                                              */
 /* ------------------------------------------------------------------ */
 /* No counterpart in the reference library.  For callers that are given

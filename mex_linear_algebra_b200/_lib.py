@@ -36,6 +36,10 @@ ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int64, C.c_int64)
 GATEWAY_ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64)
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("in_offset", C.c_int64), ("z_offset", C.c_int64)]
+
+
 class HostMatrix(C.Structure):
     _fields_ = [("kind", C.c_int32), ("sparse", C.c_int32), ("rows", C.c_int64),
                 ("cols", C.c_int64), ("data", C.c_void_p)]
@@ -72,6 +76,11 @@ SIGNATURES = {
     "mela_null_workspace_size": (_sz, [_i64, _i64]),
     "mela_dev_null_basis": (_st, [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _sz, _vp]),
     "mela_dev_unpack_rows": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
+    "mela_batch_plan_create": (_st, [C.POINTER(BatchItem), _i64, _i32, C.POINTER(_vp)]),
+    "mela_batch_plan_destroy": (None, [_vp]),
+    "mela_batch_plan_stats": (_st, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "mela_batch_rank_null": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "mela_batch_rank_null_logical": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
     "mela_static_scratch_bytes": (_sz, []),
     "mela_dev_matmul_plain_static": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp]),
 }

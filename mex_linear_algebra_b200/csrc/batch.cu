@@ -1,0 +1,854 @@
+// batch.cu -- rank and null space of many matrices in one persistent launch.
+//
+// Each matrix gets the reference's results (rank as src/mela_rank_gf2.c,
+// null-space basis as src/mela_null_gf2.c:189-274, bit for bit) from a
+// reduced row echelon form computed by one thread group:
+//
+//   class  group            storage of the matrix
+//   small  one warp         its slice of shared memory (13 KB)
+//   mid    128 threads      its slice of shared memory (55 KB)
+//   big    the whole CTA    shared memory (up to ~220 KB) or, when it does
+//          (512 threads)    not fit, the CTA's L2-resident global scratch
+//
+// The host sorts the matrices into the three classes (largest first inside
+// each class); every CTA drains the big queue, then the mid queue (4 groups),
+// then the small queue (16 warps), taking the next matrix with an atomic on
+// the class counter.  A group eliminates column by column: the rows are
+// dealt round-robin to its threads; per column each thread looks for the
+// first active row of its own holding the bit, a warp min (+ shared atomic
+// for multi-warp groups) picks the pivot, and every thread XORs the pivot row
+// into its rows holding the bit.  One group barrier per column suffices: the
+// search for column c+1 runs right after the XOR of column c on the same
+// thread's own rows.  Rows never move; the null basis is then assembled
+// directly: Zt row i = e_{f_i} + sum_p RREF(p, f_i) e_{piv(p)}.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "mela_common.cuh"
+#include "mela_internal.h"
+#include "mela_host.h"
+#include "basis.cuh"
+
+namespace mela {
+
+struct BatchDevItem {
+    int m, n;
+    int flags;  // bit 0: matrix held in shared memory
+    int pad;
+    long long in_off, z_off;
+};
+
+namespace {
+constexpr int kThreads = 512;
+constexpr int kMidGroup = 128;
+constexpr int kSmemTotal = 220 * 1024;
+constexpr int kMidBudget = kSmemTotal / (kThreads / kMidGroup);  // 55 KB
+constexpr int kSmallBudget = kSmemTotal / (kThreads / 32);       // 13.75 KB
+
+__host__ __device__ inline size_t al8(size_t x) { return (x + 7) & ~(size_t)7; }
+
+// Byte size of the per-matrix bookkeeping arrays in a group's region.
+__host__ __device__ inline size_t aux_bytes(int m, int n)
+{
+    const int wc = (n + 63) >> 6, mn = m < n ? m : n;
+    return al8((size_t)4 * (2 * (size_t)mn + (size_t)n + (size_t)wc + 1)) + 8 * (size_t)wc +
+           al8((size_t)m) + 16;
+}
+__host__ __device__ inline int smem_ld(int n)
+{
+    const int wc = (n + 63) >> 6;
+    return wc | 1;  // odd pitch: threads on consecutive rows hit different banks
+}
+}  // namespace
+
+__device__ __forceinline__ void group_sync(int G, int bar_id)
+{
+    if (G == 32) {
+        __syncwarp();
+    } else if (G == kThreads) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(G) : "memory");
+    }
+}
+
+__device__ __forceinline__ int ctz64b(u64 x) { return __ffsll((long long)x) - 1; }
+
+// RREF + null basis of one matrix by a group of G threads.
+template <int G>
+__device__ void process_matrix(const BatchDevItem &it, const u64 *__restrict__ in, u64 *__restrict__ zt,
+                               long long *ranks, int item, unsigned char *region, u64 *gmat, int gtid,
+                               int bar_id)
+{
+    const int m = it.m, n = it.n, wc = (n + 63) >> 6, mn = m < n ? m : n;
+    const bool in_smem = it.flags & 1;
+    const int ld = in_smem ? smem_ld(n) : wc;
+    u64 *A = in_smem ? reinterpret_cast<u64 *>(region) : gmat;
+    unsigned char *aux = region + (in_smem ? (size_t)m * ld * 8 : 0);
+    int *piv = reinterpret_cast<int *>(aux);
+    int *prow = piv + mn;
+    int *fcol = prow + mn;
+    int *pbase = fcol + n;
+    u64 *pm = reinterpret_cast<u64 *>(aux + al8((size_t)4 * (2 * (size_t)mn + (size_t)n + (size_t)wc + 1)));
+    unsigned char *active = reinterpret_cast<unsigned char *>(pm + wc);
+    int *slots = reinterpret_cast<int *>(active + al8((size_t)m));
+    const int lane = gtid & 31;
+
+    // load the packed matrix, mark every row active
+    const u64 *src = in + it.in_off;
+    for (long long e = gtid; e < (long long)m * wc; e += G) {
+        const int r = (int)(e / wc), x = (int)(e - (long long)r * wc);
+        A[(size_t)r * ld + x] = src[e];
+    }
+    for (int j = gtid; j < m; j += G) active[j] = 1;
+    if (gtid < 3) slots[gtid] = INT_MAX;
+    group_sync(G, bar_id);
+
+    auto search = [&](int c) {
+        if (c >= n) return;
+        const int cw = c >> 6;
+        const u64 bit = 1ull << (c & 63);
+        unsigned best = INT_MAX;
+        for (int j = gtid; j < m; j += G)
+            if (active[j] && (A[(size_t)j * ld + cw] & bit)) {
+                best = (unsigned)j;
+                break;
+            }
+        best = __reduce_min_sync(0xffffffffu, best);
+        if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&slots[c % 3], (int)best);
+    };
+
+    int r = 0;
+    search(0);
+    group_sync(G, bar_id);
+    for (int c = 0; c < n && r < m; ++c) {
+        const int p = slots[c % 3];
+        if (gtid == 0) slots[(c + 2) % 3] = INT_MAX;
+        if (p != INT_MAX) {
+            if (gtid == 0) {
+                piv[r] = c;
+                prow[r] = p;
+            }
+            if (p % G == gtid) active[p] = 0;
+            ++r;
+            const int cw = c >> 6;
+            const u64 bit = 1ull << (c & 63);
+            const u64 *pr = A + (size_t)p * ld;
+            for (int j = gtid; j < m; j += G) {
+                if (j == p) continue;
+                u64 *row = A + (size_t)j * ld;
+                if (!(row[cw] & bit)) continue;
+                for (int t = cw; t < wc; ++t) row[t] ^= pr[t];
+            }
+        }
+        search(c + 1);
+        group_sync(G, bar_id);
+    }
+    if (gtid == 0) ranks[item] = r;
+
+    // null basis: pivot mask per word, pivots before each word, free columns
+    const int f = n - r;
+    for (int W = gtid; W < wc; W += G) pm[W] = 0;
+    group_sync(G, bar_id);
+    for (int t = gtid; t < r; t += G) atomicOr(&pm[piv[t] >> 6], 1ull << (piv[t] & 63));
+    group_sync(G, bar_id);
+    if (gtid == 0) {
+        int pc = 0, fc = 0;
+        for (int W = 0; W < wc; ++W) {
+            pbase[W] = pc;
+            pc += __popcll(pm[W]);
+            const int valid = n - 64 * W;
+            const u64 vm = valid >= 64 ? ~0ull : ((1ull << valid) - 1);
+            u64 fm = ~pm[W] & vm;
+            while (fm) {
+                fcol[fc++] = 64 * W + ctz64b(fm);
+                fm &= fm - 1;
+            }
+        }
+        pbase[wc] = pc;
+    }
+    group_sync(G, bar_id);
+    u64 *Z = zt + it.z_off;
+    for (long long e = gtid; e < (long long)f * wc; e += G) {
+        const int i = (int)(e / wc), W = (int)(e - (long long)i * wc);
+        const int fi = fcol[i], fw = fi >> 6, fb = fi & 63;
+        u64 out = (fw == W) ? (1ull << fb) : 0ull;
+        for (int q = pbase[W]; q < pbase[W + 1]; ++q)
+            out |= ((A[(size_t)prow[q] * ld + fw] >> fb) & 1ull) << (piv[q] & 63);
+        Z[e] = out;
+    }
+    group_sync(G, bar_id);
+}
+
+// ---------------------------------------------------------------- big matrices
+// Global-scratch layout (words) of one big matrix: A (m x wc), then the
+// arrays that do not fit in shared memory.  See big_layout().
+struct BigLayout {
+    long long A, Rg, ysg, yvg, tagg, ints, pm, active, rt, q, total;  // word offsets
+};
+
+__host__ __device__ inline BigLayout big_layout(long long m, long long n)
+{
+    const long long wc = (n + 63) / 64, mn = m < n ? m : n;
+    BigLayout L;
+    long long o = 0;
+    L.A = o; o += m * wc;
+    L.Rg = o; o += 128 * wc;          // stage + reduced rows when shared memory is short
+    L.ysg = o; o += m;
+    L.yvg = o; o += m;
+    L.tagg = o; o += m;
+    L.ints = o; o += (2 * mn + 2 * n + wc + 2 + 1) / 2 + 1;  // piv, prow, fcol, cmap, pbase
+    L.pm = o; o += wc;
+    L.active = o; o += (m + 7) / 8;
+    L.rt = o; o += (n * ((mn + 31) / 32) + 1) / 2 + 1;      // R^T, 32-bit words
+    L.q = o; o += (mn * ((n + 31) / 32) + 1) / 2 + 1;       // (R restricted to free columns)
+    L.total = o + 8;
+    return L;
+}
+__host__ __device__ inline long long big_scratch_words(long long m, long long n)
+{
+    return big_layout(m, n).total;
+}
+
+namespace {
+constexpr int kBigWarps = kThreads / 32;
+constexpr int kTW = 32;  // words per update chunk (one per lane)
+struct BigSmem {
+    u64 coef[64];
+    int bits[64], srow[64];
+    int slots[4];
+    u64 T[16][16][kTW];  // nibble tables of the current chunk
+    u64 pm;
+    int p;
+};
+// Shared memory after BigSmem: panel stage + reduced rows, then the per-row
+// panel words (snapshot, working copy, combination tags), when they fit.
+constexpr size_t kBigExtra = (size_t)kSmemTotal - ((sizeof(BigSmem) + 15) & ~(size_t)15);
+static_assert(sizeof(BigSmem) <= (size_t)kSmemTotal, "big-matrix shared memory");
+}  // namespace
+
+// 32x32 bit transposes by warp ballots over a CTA: dst (cols x rows bits,
+// 32-bit words, pitch dld) = src^T, where src row r, 32-bit word x is
+// srcw(r, x) (rows x cols bits).
+template <typename F>
+__device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dld)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5;
+    for (long long t = warp; t < (long long)rt * ct; t += kBigWarps) {
+        const int tr = (int)(t / ct), tc = (int)(t - (long long)tr * ct);
+        const int r = tr * 32 + lane;
+        const u32 x = r < rows ? srcw(r, tc) : 0u;
+        u32 keep = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+            const u32 v = __ballot_sync(0xffffffffu, (x >> b) & 1u);
+            if (lane == b) keep = v;
+        }
+        const int c = tc * 32 + lane;
+        if (c < cols) dst[(long long)c * dld + tr] = keep;
+    }
+}
+
+// Reduced row echelon form and null basis of a big matrix by the whole CTA,
+// 64 columns at a time (the blocked form of elim.cu inside one CTA):
+//  * pivot selection: per bit of the panel, the first active row holding it
+//    becomes a pivot and is XORed into every other row holding it -- on the
+//    panel words only, each row carrying a 64-bit tag of the pivots folded
+//    into it, so pivot k's reduced row is its original row plus the original
+//    pivot rows of its tag (one barrier per bit);
+//  * the reduced pivot rows R_k are formed from the staged original rows and
+//    written over them; every other row is updated with 16 nibble-table
+//    lookups per word (tables of the 16 combinations of 4 reduced rows),
+//    a warp per row so that global accesses are contiguous;
+//  * null basis: Zt = (Y)^T with Y row c = (R restricted to free columns)^T
+//    row p when c is pivot column p, the unit vector of its free index
+//    otherwise -- three 32x32 ballot transposes, no per-bit gathers.
+__device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restrict__ in,
+                                    u64 *__restrict__ zt, long long *ranks, int item,
+                                    unsigned char *smem_raw, u64 *g)
+{
+    BigSmem &S = *reinterpret_cast<BigSmem *>(smem_raw);
+    const int m = it.m, n = it.n, wc = (n + 63) >> 6, mn = m < n ? m : n;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const BigLayout L = big_layout(m, n);
+    u64 *A = g + L.A;
+    int *piv = reinterpret_cast<int *>(g + L.ints);
+    int *prow = piv + mn;
+    int *fcol = prow + mn;
+    int *cmap = fcol + n;
+    int *pbase = cmap + n;
+    u64 *pm = g + L.pm;
+    u32 *Rt = reinterpret_cast<u32 *>(g + L.rt);
+    u32 *Q = reinterpret_cast<u32 *>(g + L.q);
+
+    unsigned char *extra = smem_raw + ((sizeof(BigSmem) + 15) & ~(size_t)15);
+    const size_t rb_bytes = (size_t)64 * wc * 8, row_bytes = (size_t)m * 8;
+    const bool r_in_smem = 2 * rb_bytes <= kBigExtra;
+    u64 *stage = r_in_smem ? reinterpret_cast<u64 *>(extra) : g + L.Rg;
+    u64 *Rbuf = stage + (size_t)64 * wc;
+    size_t used = r_in_smem ? 2 * rb_bytes : 0;
+    // row states are read on every bit step: shared memory whenever possible
+    const size_t act_bytes = ((size_t)m + 15) & ~(size_t)15;
+    unsigned char *active = (used + act_bytes <= kBigExtra) ? extra + used
+                                                           : reinterpret_cast<unsigned char *>(g + L.active);
+    if (used + act_bytes <= kBigExtra) used += act_bytes;
+    const bool rows_in_smem = used + 3 * row_bytes <= kBigExtra;
+    u64 *ysnap = rows_in_smem ? reinterpret_cast<u64 *>(extra + used) : g + L.ysg;
+    u64 *yv = rows_in_smem ? ysnap + m : g + L.yvg;
+    u64 *tag = rows_in_smem ? yv + m : g + L.tagg;
+
+    const u64 *src = in + it.in_off;
+    for (long long e = tid; e < (long long)m * wc; e += kThreads) A[e] = src[e];
+    for (int j = tid; j < m; j += kThreads) active[j] = 1;
+    __syncthreads();
+
+    int r = 0;
+    for (int w = 0; w < wc && r < m; ++w) {
+        // 1. panel words, pivot search for bit 0
+        if (tid < 3) S.slots[tid] = INT_MAX;
+        __syncthreads();
+        unsigned best = INT_MAX;
+        for (int j = tid; j < m; j += kThreads) {
+            const u64 word = A[(size_t)j * wc + w];
+            ysnap[j] = word;
+            const u64 y = active[j] == 1 ? word : 0ull;
+            yv[j] = y;
+            tag[j] = 0;
+            if ((y & 1ull) && best == (unsigned)INT_MAX) best = j;
+        }
+        best = __reduce_min_sync(0xffffffffu, best);
+        if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[0], (int)best);
+        __syncthreads();
+        // 2. per-bit elimination of the panel words with combination tags
+        int k = 0;
+        u64 pmask = 0;
+        for (int b = 0; b < 64; ++b) {
+            const int p = S.slots[b % 3];
+            if (tid == 0) S.slots[(b + 2) % 3] = INT_MAX;
+            if (p != INT_MAX) {
+                const u64 yp = yv[p], tp = tag[p] ^ (1ull << k);
+                if (tid == 0) {
+                    S.bits[k] = b;
+                    S.srow[k] = p;
+                }
+                if (p % kThreads == tid) active[p] = 2;
+                const u64 bit = 1ull << b;
+                for (int j = tid; j < m; j += kThreads) {
+                    if (j == p || active[j] == 0) continue;
+                    if (yv[j] & bit) {
+                        yv[j] ^= yp;
+                        tag[j] ^= tp;
+                    }
+                }
+                pmask |= bit;
+                ++k;
+            }
+            if (b < 63) {
+                const u64 bit = 1ull << (b + 1);
+                best = INT_MAX;
+                for (int j = tid; j < m; j += kThreads)
+                    if (active[j] == 1 && (yv[j] & bit)) {
+                        best = j;
+                        break;
+                    }
+                best = __reduce_min_sync(0xffffffffu, best);
+                if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[(b + 1) % 3], (int)best);
+            }
+            __syncthreads();
+        }
+        const int p = k;
+        if (p == 0) continue;
+        for (int t = tid; t < p; t += kThreads) {
+            S.coef[t] = tag[S.srow[t]] ^ (1ull << t);
+            piv[r + t] = 64 * w + S.bits[t];
+            prow[r + t] = S.srow[t];
+        }
+        const int rem = wc - w;
+        // 3. reduced pivot rows from the staged original rows
+        __syncthreads();
+        for (int e = tid; e < p * rem; e += kThreads) {
+            const int i = e / rem, x = w + e % rem;
+            stage[(size_t)i * wc + x] = A[(size_t)S.srow[i] * wc + x];
+        }
+        __syncthreads();
+        for (int e = tid; e < p * rem; e += kThreads) {
+            const int kk = e / rem, x = w + e % rem;
+            u64 c = S.coef[kk], v = 0;
+            while (c) {
+                const int i = ctz64_(c);
+                c &= c - 1;
+                v ^= stage[(size_t)i * wc + x];
+            }
+            Rbuf[(size_t)kk * wc + x] = v;
+            A[(size_t)S.srow[kk] * wc + x] = v;
+        }
+        __syncthreads();
+        // 4. update every other row, 32 words at a time
+        for (int x0 = w; x0 < wc; x0 += kTW) {
+            for (int e = tid; e < 16 * 5 * kTW; e += kThreads) {
+                const int t = e % kTW, gh = e / kTW, gi = gh / 5, h = gh % 5;
+                if (h == 4) {
+                    S.T[gi][0][t] = 0;
+                    continue;
+                }
+                const int bb = 4 * gi + h, x = x0 + t;
+                u64 v = 0;
+                if (((pmask >> bb) & 1) && x < wc) {
+                    const int kk = __popcll(pmask & ((1ull << bb) - 1));
+                    v = Rbuf[(size_t)kk * wc + x];
+                }
+                S.T[gi][1 << h][t] = v;
+            }
+            __syncthreads();
+            for (int h = 1; h < 4; ++h) {
+                const int cnt = (1 << h) - 1;
+                for (int e = tid; e < 16 * cnt * kTW; e += kThreads) {
+                    const int t = e % kTW, rest = e / kTW, gi = rest / cnt, v = (1 << h) + 1 + rest % cnt;
+                    S.T[gi][v][t] = S.T[gi][v - (1 << h)][t] ^ S.T[gi][1 << h][t];
+                }
+                __syncthreads();
+            }
+            const int x = x0 + lane;
+            const int warp = tid >> 5;
+            for (int j0 = warp * 4; j0 < m; j0 += kBigWarps * 4) {
+                u64 y[4], a[4];
+                bool go[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j = j0 + q;
+                    go[q] = false;
+                    y[q] = 0;
+                    if (j < m && active[j] != 2) {
+                        y[q] = ysnap[j] & pmask;
+                        go[q] = y[q] != 0 && x < wc;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (go[q]) a[q] = A[(size_t)(j0 + q) * wc + x];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!go[q]) continue;
+                    u64 acc = 0;
+#pragma unroll
+                    for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][lane];
+                    A[(size_t)(j0 + q) * wc + x] = a[q] ^ acc;
+                }
+            }
+            __syncthreads();
+        }
+        for (int t = tid; t < p; t += kThreads) active[S.srow[t]] = 0;
+        r += p;
+        __syncthreads();
+    }
+    if (tid == 0) ranks[item] = r;
+
+    // ---- null basis
+    const int f = n - r;
+    for (int W = tid; W < wc; W += kThreads) pm[W] = 0;
+    for (int c = tid; c < n; c += kThreads) cmap[c] = -1;
+    __syncthreads();
+    for (int t = tid; t < r; t += kThreads) {
+        atomicOr(&pm[piv[t] >> 6], 1ull << (piv[t] & 63));
+        cmap[piv[t]] = t;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int pc = 0;
+        for (int W = 0; W < wc; ++W) {
+            pbase[W] = pc;
+            pc += __popcll(pm[W]);
+        }
+        pbase[wc] = pc;
+    }
+    __syncthreads();
+    // free columns: word W's free bits go to ranks [64W - pbase[W], ...)
+    for (int W = tid; W < wc; W += kThreads) {
+        const int valid = n - 64 * W;
+        const u64 vm = valid >= 64 ? ~0ull : ((1ull << valid) - 1);
+        u64 fm = ~pm[W] & vm;
+        int fc = 64 * W - pbase[W];
+        while (fm) {
+            const int c = 64 * W + ctz64_(fm);
+            fcol[fc] = c;
+            cmap[c] = -(fc + 1);
+            ++fc;
+            fm &= fm - 1;
+        }
+    }
+    __syncthreads();
+    if (f == 0) return;
+    const int rt32 = (r + 31) >> 5, q32 = (f + 31) >> 5;
+    if (r > 0) {
+        // Rt (n x r) = R^T, R row p = A[prow[p]]
+        cta_transpose([&](int row, int x) -> u32 {
+            return reinterpret_cast<const u32 *>(A + (size_t)prow[row] * wc)[x];
+        }, r, n, Rt, rt32);
+        __syncthreads();
+        // Q (r x f) = (rows f_i of Rt)^T: row p = RREF row p at the free columns
+        cta_transpose([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
+                      f, r, Q, q32);
+        __syncthreads();
+    }
+    // Zt (f x n) = Y^T, Y row c = Q row p (pivot column c) or e_i (free column i)
+    u64 *Z = zt + it.z_off;
+    u32 *Z32 = reinterpret_cast<u32 *>(Z);
+    if ((n & 63) && (n & 63) <= 32)
+        for (int i = tid; i < f; i += kThreads) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
+    cta_transpose([&](int c, int y) -> u32 {
+        const int mc = cmap[c];
+        if (mc >= 0) return Q[(long long)mc * q32 + y];
+        const int fi = -mc - 1;
+        return ((fi >> 5) == y) ? (1u << (fi & 31)) : 0u;
+    }, n, f, Z32, 2LL * wc);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+batch_kernel(const BatchDevItem *__restrict__ items, const int *__restrict__ order, int n_big,
+             int n_mid, int n_small, int *counters, const u64 *__restrict__ in, u64 *__restrict__ zt,
+             long long *ranks, u64 *gscratch, long long gscratch_words)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_next[kThreads / 32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    u64 *gmat = gscratch + (long long)blockIdx.x * gscratch_words;
+
+    // big: the whole CTA per matrix
+    while (true) {
+        if (tid == 0) s_next[0] = atomicAdd(&counters[0], 1);
+        __syncthreads();
+        const int k = s_next[0];
+        __syncthreads();
+        if (k >= n_big) break;
+        const int item = order[k];
+        process_big_blocked(items[item], in, zt, ranks, item, smem, gmat);
+    }
+    // mid: four groups of 128 threads, each with a quarter of shared memory
+    {
+        const int g = tid / kMidGroup, gtid = tid % kMidGroup;
+        unsigned char *region = smem + (size_t)g * kMidBudget;
+        while (true) {
+            if (gtid == 0) s_next[g] = atomicAdd(&counters[1], 1);
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kMidGroup) : "memory");
+            const int k = s_next[g];
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kMidGroup) : "memory");
+            if (k >= n_mid) break;
+            const int item = order[n_big + k];
+            process_matrix<kMidGroup>(items[item], in, zt, ranks, item, region, nullptr, gtid, 1 + g);
+        }
+    }
+    __syncthreads();
+    // small: one warp per matrix
+    {
+        unsigned char *region = smem + (size_t)warp * kSmallBudget;
+        while (true) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&counters[2], 1);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            if (k >= n_small) break;
+            const int item = order[n_big + n_mid + k];
+            process_matrix<32>(items[item], in, zt, ranks, item, region, nullptr, lane, 0);
+        }
+    }
+}
+
+// logical column-major inputs -> packed rows, for every matrix of the batch
+__global__ void batch_pack_kernel(const BatchDevItem *__restrict__ items, const long long *byte_off,
+                                  const long long *tile_start, int count,
+                                  const unsigned char *__restrict__ in, u64 *__restrict__ out)
+{
+    // one block = 32 rows x 8 words of one matrix; find the matrix by binary search
+    const long long b = blockIdx.x;
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const BatchDevItem it = items[lo];
+    const long long tile = b - tile_start[lo];
+    const int wc = (it.n + 63) >> 6, wg = (wc + 7) / 8;
+    const int rt = (int)(tile / wg), wt = (int)(tile % wg);
+    const int lane = threadIdx.x & 31, w8 = threadIdx.x >> 5;
+    const int row = rt * 32 + lane, w = wt * 8 + w8;
+    if (row >= it.m || w >= wc) return;
+    const unsigned char *p = in + byte_off[lo] + row + (long long)w * 64 * it.m;
+    const int cols = (it.n - w * 64) < 64 ? (it.n - w * 64) : 64;
+    u64 word = 0;
+    for (int j = 0; j < cols; ++j) word |= (u64)(p[(long long)j * it.m] != 0) << j;
+    out[it.in_off + (long long)row * wc + w] = word;
+}
+
+// ---------------------------------------------------------------- host side
+struct BatchPlanImpl {
+    int count = 0, n_big = 0, n_mid = 0, n_small = 0;
+    BatchDevItem *d_items = nullptr;
+    int *d_order = nullptr;
+    int *d_counters = nullptr;
+    u64 *d_gscratch = nullptr;
+    long long gscratch_words = 0;
+    int grid = 0;
+    // logical-input path
+    long long *d_byte_off = nullptr, *d_tile_start = nullptr;
+    long long pack_tiles = 0;
+    u64 *d_packed = nullptr;
+    long long packed_words = 0;
+    // CUDA graph of the last run
+    cudaGraphExec_t exec = nullptr;
+    const void *g_in = nullptr;
+    void *g_zt = nullptr, *g_ranks = nullptr;
+    int g_logical = -1;
+    cudaStream_t cap_stream = nullptr;  // private stream the graph is captured on
+    // statistics
+    long long class_count[3] = {0, 0, 0};
+};
+
+static mela_status plan_free(BatchPlanImpl *P)
+{
+    if (!P) return MELA_OK;
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+    cudaFree(P->d_items);
+    cudaFree(P->d_order);
+    cudaFree(P->d_counters);
+    cudaFree(P->d_gscratch);
+    cudaFree(P->d_byte_off);
+    cudaFree(P->d_tile_start);
+    cudaFree(P->d_packed);
+    delete P;
+    return MELA_OK;
+}
+
+static mela_status plan_create(const mela_batch_item *h, long long count, int force_class,
+                               BatchPlanImpl **out)
+{
+    *out = nullptr;
+    if (count < 0 || (count > 0 && !h) || count > INT_MAX) {
+        set_error("batch: bad item list");
+        return MELA_ERR_INVALID;
+    }
+    BatchPlanImpl *P = new BatchPlanImpl();
+    P->count = (int)count;
+    std::vector<BatchDevItem> items((size_t)count);
+    std::vector<int> cls((size_t)count);
+    std::vector<double> cost((size_t)count);
+    long long max_big_words = 0;
+    for (long long i = 0; i < count; ++i) {
+        const long long m = h[i].m, n = h[i].n;
+        if (m < 0 || n < 0 || m > INT_MAX / 2 || n > INT_MAX / 2 || h[i].in_offset < 0 || h[i].z_offset < 0) {
+            plan_free(P);
+            set_error("batch: item %lld has a bad shape or offset", i);
+            return MELA_ERR_INVALID;
+        }
+        BatchDevItem d{};
+        d.m = (int)m;
+        d.n = (int)n;
+        d.in_off = h[i].in_offset;
+        d.z_off = h[i].z_offset;
+        const size_t aux = aux_bytes((int)m, (int)n);
+        const size_t mat = (size_t)m * smem_ld((int)n) * 8;
+        int c;
+        if (aux + mat <= (size_t)kSmallBudget && m <= 256) c = 2;
+        else if (aux + mat <= (size_t)kMidBudget) c = 1;
+        else c = 0;
+        if (force_class >= 0 && force_class <= 2) {
+            // a forced class must still fit its region; otherwise fall back to big
+            const size_t budget = force_class == 2 ? kSmallBudget : force_class == 1 ? kMidBudget : kSmemTotal;
+            if (force_class == 0 || aux + mat <= budget) c = force_class;
+        }
+        if (c == 0) {
+            d.flags = 0;  // big matrices live in the CTA's global scratch
+            max_big_words = std::max(max_big_words, big_scratch_words(m, n));
+        } else {
+            d.flags = 1;
+        }
+        items[(size_t)i] = d;
+        cls[(size_t)i] = c;
+        cost[(size_t)i] = (double)m * (double)n * (double)((n + 63) / 64);
+        P->class_count[c]++;
+    }
+    std::vector<int> order((size_t)count);
+    for (int i = 0; i < (int)count; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (cls[(size_t)a] != cls[(size_t)b]) return cls[(size_t)a] < cls[(size_t)b];
+        return cost[(size_t)a] > cost[(size_t)b];
+    });
+    P->n_big = (int)P->class_count[0];
+    P->n_mid = (int)P->class_count[1];
+    P->n_small = (int)P->class_count[2];
+    P->grid = sm_count();
+    P->gscratch_words = max_big_words;
+
+    // logical-input packing tiles
+    std::vector<long long> byte_off((size_t)count), tiles((size_t)count);
+    long long boff = 0, t = 0;
+    for (long long i = 0; i < count; ++i) {
+        byte_off[(size_t)i] = boff;
+        boff += h[i].m * h[i].n;
+        tiles[(size_t)i] = t;
+        const long long wc = (h[i].n + 63) / 64;
+        t += ((h[i].m + 31) / 32) * ((wc + 7) / 8);
+        P->packed_words = std::max(P->packed_words, h[i].in_offset + h[i].m * wc);
+    }
+    P->pack_tiles = t;
+
+    auto dmal = [&](void **p, size_t bytes) -> mela_status {
+        cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (batch plan)");
+        return MELA_OK;
+    };
+    mela_status st;
+    if ((st = dmal((void **)&P->d_items, items.size() * sizeof(BatchDevItem))) != MELA_OK ||
+        (st = dmal((void **)&P->d_order, order.size() * sizeof(int))) != MELA_OK ||
+        (st = dmal((void **)&P->d_counters, 4 * sizeof(int))) != MELA_OK ||
+        (st = dmal((void **)&P->d_gscratch, (size_t)P->grid * (size_t)max_big_words * 8)) != MELA_OK ||
+        (st = dmal((void **)&P->d_byte_off, byte_off.size() * 8)) != MELA_OK ||
+        (st = dmal((void **)&P->d_tile_start, tiles.size() * 8)) != MELA_OK) {
+        plan_free(P);
+        return st;
+    }
+    cudaMemcpy(P->d_items, items.data(), items.size() * sizeof(BatchDevItem), cudaMemcpyHostToDevice);
+    cudaMemcpy(P->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(P->d_byte_off, byte_off.data(), byte_off.size() * 8, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(P->d_tile_start, tiles.data(), tiles.size() * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        plan_free(P);
+        return cuda_status(e, "batch plan upload");
+    }
+    *out = P;
+    return MELA_OK;
+}
+
+static mela_status enqueue(BatchPlanImpl *P, const u64 *in, u64 *zt, long long *ranks, cudaStream_t s)
+{
+    MELA_CUDA_TRY(cudaMemsetAsync(P->d_counters, 0, 4 * sizeof(int), s));
+    if (P->count == 0) return MELA_OK;
+    batch_kernel<<<P->grid, kThreads, kSmemTotal, s>>>(P->d_items, P->d_order, P->n_big, P->n_mid,
+                                                       P->n_small, P->d_counters, in, zt, ranks,
+                                                       P->d_gscratch, P->gscratch_words);
+    MELA_LAUNCH_CHECK("batch_kernel");
+    return MELA_OK;
+}
+
+static mela_status enqueue_logical(BatchPlanImpl *P, const unsigned char *in, u64 *zt, long long *ranks,
+                                   cudaStream_t s)
+{
+    if (P->count && P->pack_tiles) {
+        batch_pack_kernel<<<(unsigned)P->pack_tiles, 256, 0, s>>>(P->d_items, P->d_byte_off,
+                                                                   P->d_tile_start, P->count, in,
+                                                                   P->d_packed);
+        MELA_LAUNCH_CHECK("batch_pack_kernel");
+    }
+    return enqueue(P, P->d_packed, zt, ranks, s);
+}
+
+static mela_status run(BatchPlanImpl *P, const void *in, int logical, u64 *zt, long long *ranks,
+                       cudaStream_t s, int use_graph)
+{
+    static bool attr = false;
+    if (!attr) {
+        MELA_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemTotal));
+        attr = true;
+    }
+    if (logical && !P->d_packed) {
+        cudaError_t e = cudaMalloc((void **)&P->d_packed, (size_t)(P->packed_words ? P->packed_words : 1) * 8);
+        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (batch packed buffer)");
+    }
+    if (!use_graph) {
+        return logical ? enqueue_logical(P, (const unsigned char *)in, zt, ranks, s)
+                       : enqueue(P, (const u64 *)in, zt, ranks, s);
+    }
+    if (!P->exec || P->g_in != in || P->g_zt != zt || P->g_ranks != ranks ||
+        P->g_logical != logical) {
+        if (P->exec) {
+            cudaGraphExecDestroy(P->exec);
+            P->exec = nullptr;
+        }
+        // Captured on a private stream (the caller's may be the legacy default
+        // stream, which cannot be captured); launched on the caller's stream.
+        if (!P->cap_stream) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking));
+        const cudaStream_t cs = P->cap_stream;
+        cudaGraph_t g;
+        MELA_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        mela_status st = logical ? enqueue_logical(P, (const unsigned char *)in, zt, ranks, cs)
+                                 : enqueue(P, (const u64 *)in, zt, ranks, cs);
+        cudaError_t e = cudaStreamEndCapture(cs, &g);
+        if (st != MELA_OK) return st;
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&P->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+        P->g_in = in;
+        P->g_zt = zt;
+        P->g_ranks = ranks;
+        P->g_logical = logical;
+    }
+    MELA_CUDA_TRY(cudaGraphLaunch(P->exec, s));
+    return MELA_OK;
+}
+
+}  // namespace mela
+
+using namespace mela;
+
+struct mela_batch_plan {
+    BatchPlanImpl *impl;
+};
+
+extern "C" mela_status mela_batch_plan_create(const mela_batch_item *items, int64_t count,
+                                              int32_t force_class, mela_batch_plan **plan)
+{
+    if (!plan) {
+        set_error("null plan pointer");
+        return MELA_ERR_INVALID;
+    }
+    *plan = nullptr;
+    BatchPlanImpl *P = nullptr;
+    mela_status st = plan_create(items, count, force_class, &P);
+    if (st != MELA_OK) return st;
+    *plan = new mela_batch_plan{P};
+    return MELA_OK;
+}
+
+extern "C" void mela_batch_plan_destroy(mela_batch_plan *plan)
+{
+    if (!plan) return;
+    plan_free(plan->impl);
+    delete plan;
+}
+
+extern "C" mela_status mela_batch_plan_stats(const mela_batch_plan *plan, int64_t *big, int64_t *mid,
+                                             int64_t *small)
+{
+    if (!plan) return MELA_ERR_INVALID;
+    if (big) *big = plan->impl->class_count[0];
+    if (mid) *mid = plan->impl->class_count[1];
+    if (small) *small = plan->impl->class_count[2];
+    return MELA_OK;
+}
+
+extern "C" mela_status mela_batch_rank_null(mela_batch_plan *plan, const uint64_t *d_in,
+                                            uint64_t *d_zt, int64_t *d_ranks, int32_t use_graph,
+                                            void *stream)
+{
+    if (!plan || (plan->impl->count && (!d_in || !d_zt || !d_ranks))) {
+        set_error("mela_batch_rank_null: null argument");
+        return MELA_ERR_INVALID;
+    }
+    return run(plan->impl, d_in, 0, (u64 *)d_zt, (long long *)d_ranks, (cudaStream_t)stream, use_graph);
+}
+
+extern "C" mela_status mela_batch_rank_null_logical(mela_batch_plan *plan, const uint8_t *d_in,
+                                                    uint64_t *d_zt, int64_t *d_ranks,
+                                                    int32_t use_graph, void *stream)
+{
+    if (!plan || (plan->impl->count && (!d_in || !d_zt || !d_ranks))) {
+        set_error("mela_batch_rank_null_logical: null argument");
+        return MELA_ERR_INVALID;
+    }
+    return run(plan->impl, d_in, 1, (u64 *)d_zt, (long long *)d_ranks, (cudaStream_t)stream, use_graph);
+}

@@ -40,11 +40,12 @@
 #include "mela_internal.h"
 #include "mela_host.h"
 #include "elim.h"
+#include "basis.cuh"
 
 namespace mela {
 
 // ---------------------------------------------------------------- helpers
-__device__ __forceinline__ int ctz64(u64 x) { return __ffsll((long long)x) - 1; }
+__device__ __forceinline__ int ctz64(u64 x) { return ctz64_(x); }
 
 // Panel bookkeeping shared by the three blocked kernels (device memory).
 struct PanelState {
@@ -61,40 +62,11 @@ struct PanelState {
 namespace {
 constexpr int SEL_WARPS = 32;
 struct SelSmem {
-    u64 B[SEL_WARPS][64];   // reduced basis vectors, indexed by leading bit
-    u64 O[SEL_WARPS][64];   // original words of the rows that entered the basis
-    int R[SEL_WARPS][64];   // their physical rows
+    WarpBasis wb[SEL_WARPS];
     u64 have[SEL_WARPS];
+    int bits[64];
 };
 }  // namespace
-
-// Insert the lane values x (original word o, row r) into the warp basis `wb`.
-__device__ void warp_insert(SelSmem &sm, int wb, u64 x, u64 o, int r, u64 &have)
-{
-    const int lane = threadIdx.x & 31;
-    while (true) {
-        while (x) {
-            const u64 lb = x & (~x + 1);
-            if (!(lb & have)) break;
-            x ^= sm.B[wb][ctz64(lb)];
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, x != 0);
-        if (!bal) break;
-        const int src = __ffs(bal) - 1;
-        const u64 xb = __shfl_sync(0xffffffffu, x, src);
-        const u64 ob = __shfl_sync(0xffffffffu, o, src);
-        const int rb = __shfl_sync(0xffffffffu, r, src);
-        const int b = ctz64(xb);
-        if (lane == 0) {
-            sm.B[wb][b] = xb;
-            sm.O[wb][b] = ob;
-            sm.R[wb][b] = rb;
-        }
-        have |= 1ull << b;
-        if (lane == src) x = 0;
-        __syncwarp();
-    }
-}
 
 __global__ void __launch_bounds__(1024, 1)
 panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned char *state,
@@ -115,25 +87,13 @@ panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned ch
             ysnap[j] = word;
             if (state[j]) x = word;
         }
-        warp_insert(sm, wi, x, x, (int)j, have);
+        warp_basis_insert(sm.wb[wi], x, x, (int)j, have);
     }
     if (lane == 0) sm.have[wi] = have;
     for (int step = 1; step < SEL_WARPS; step <<= 1) {
         __syncthreads();
         if ((wi % (2 * step)) == 0 && wi + step < SEL_WARPS) {
-            const int other = wi + step;
-            const u64 oh = sm.have[other];
-            // two batches of 32 candidates: the other basis' leading bits
-            for (int half = 0; half < 2; ++half) {
-                const int b = half * 32 + lane;
-                u64 o = 0;
-                int r = 0;
-                if ((oh >> b) & 1) {
-                    o = sm.O[other][b];
-                    r = sm.R[other][b];
-                }
-                warp_insert(sm, wi, o, o, r, have);
-            }
+            warp_basis_merge(sm.wb[wi], have, sm.wb[wi + step], sm.have[wi + step]);
             if (lane == 0) sm.have[wi] = have;
         }
     }
@@ -141,76 +101,14 @@ panel_select_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 w, unsigned ch
     if (wi != 0) return;
 
     const u64 pm = have;
-    const int p = __popcll(pm);
     const long long r0 = ps->rank;
-    if (p == 0) {
-        if (lane == 0) {
-            ps->p = 0;
-            ps->pivmask = 0;
-        }
-        return;
-    }
-    // rows k = 0..p-1 in increasing leading bit; lane holds k = lane and lane + 32
-    u64 q[2], a[2];
-    int rowk[2];
-    bool used[2] = {false, false};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int k = lane + 32 * h;
-        q[h] = 0;
-        a[h] = 0;
-        rowk[h] = -1;
-        if (k < p) {
-            // bit position of the k-th set bit of pm
-            u64 t = pm;
-            for (int i = 0; i < k; ++i) t &= t - 1;
-            const int b = ctz64(t);
-            q[h] = sm.O[0][b] & pm;
-            a[h] = 1ull << k;
-            rowk[h] = sm.R[0][b];
-        }
-    }
-    // Gauss-Jordan over the pivot bits, increasing.  The row chosen at step t
-    // keeps being reduced by later steps, so its combination is final only
-    // after the loop.
-    int step[2] = {-1, -1};
-    u64 rest = pm;
-    for (int t = 0; t < p; ++t) {
-        const int b = ctz64(rest);
-        rest &= rest - 1;
-        const u64 bit = 1ull << b;
-        const unsigned c0 = __ballot_sync(0xffffffffu, !used[0] && (q[0] & bit));
-        const unsigned c1 = __ballot_sync(0xffffffffu, !used[1] && (q[1] & bit));
-        const int src = c0 ? (__ffs(c0) - 1) : (__ffs(c1) - 1);
-        const int sh = c0 ? 0 : 1;
-        const u64 qs = __shfl_sync(0xffffffffu, sh ? q[1] : q[0], src);
-        const u64 as = __shfl_sync(0xffffffffu, sh ? a[1] : a[0], src);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const bool me = (lane == src && h == sh);
-            if (!me && (q[h] & bit)) {
-                q[h] ^= qs;
-                a[h] ^= as;
-            }
-            if (me) {
-                used[h] = true;
-                step[h] = t;
-            }
-        }
-        if (lane == 0) piv[r0 + t] = 64 * w + b;
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int k = lane + 32 * h;
-        if (k < p) {
-            const int t = step[h];
-            ps->sel[k] = rowk[h];
-            ps->coef[t] = a[h];
-            ps->srow[t] = rowk[h];
-            prow[r0 + t] = rowk[h];
-            state[rowk[h]] = 0;
-            stamp[rowk[h]] = panel;
-        }
+    const int p = warp_panel_gauss_jordan(sm.wb[0], pm, sm.bits, ps->coef, ps->srow, ps->sel);
+    for (int t = lane; t < p; t += 32) {
+        const int rs = ps->srow[t];
+        piv[r0 + t] = 64 * w + sm.bits[t];
+        prow[r0 + t] = rs;
+        state[rs] = 0;
+        stamp[rs] = panel;
     }
     if (lane == 0) {
         ps->p = p;

@@ -87,3 +87,79 @@ def device_error_flags(clear: bool = True) -> int:
     v = C.c_uint32(0)
     check(lib().mela_device_error_flags(C.byref(v), 1 if clear else 0))
     return int(v.value)
+
+
+class BatchPlan:
+    """Batched rank + null space (mela_batch_* entry points).
+
+    ``shapes``: sequence of (m, n).  Inputs are packed back to back in the
+    order given (``in_offsets``, words); the null-space bases come back in a
+    buffer with room for n rows of ceil(n/64) words per matrix
+    (``z_offsets``).
+    """
+
+    def __init__(self, shapes, force_class: int = -1):
+        import ctypes as C
+        import numpy as np
+        self.shapes = np.asarray(shapes, dtype=np.int64).reshape(-1, 2)
+        m, n = self.shapes[:, 0], self.shapes[:, 1]
+        wc = (n + 63) // 64
+        self.wc = wc
+        sizes = m * wc
+        self.in_offsets = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        zsz = n * wc
+        self.z_offsets = np.concatenate([[0], np.cumsum(zsz)[:-1]]).astype(np.int64)
+        self.in_words = int(sizes.sum())
+        self.z_words = int(zsz.sum())
+        self.logical_bytes = int((m * n).sum())
+        cnt = len(self.shapes)
+        items = (_lib.BatchItem * max(cnt, 1))()
+        for i in range(cnt):
+            items[i] = _lib.BatchItem(int(m[i]), int(n[i]), int(self.in_offsets[i]), int(self.z_offsets[i]))
+        self._plan = C.c_void_p()
+        check(lib().mela_batch_plan_create(items, cnt, force_class, C.byref(self._plan)))
+        self.count = cnt
+
+    def stats(self):
+        import ctypes as C
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mela_batch_plan_stats(self._plan, C.byref(a), C.byref(b), C.byref(c)))
+        return {"cta": a.value, "group128": b.value, "warp": c.value}
+
+    def outputs(self, device="cuda"):
+        ranks = torch.empty(max(self.count, 1), dtype=torch.int64, device=device)
+        zt = torch.empty(max(self.z_words, 1), dtype=torch.int64, device=device)
+        return ranks, zt
+
+    def run(self, d_in, ranks=None, zt=None, use_graph: bool = True, stream=None):
+        if ranks is None:
+            ranks, zt = self.outputs(d_in.device)
+        check(lib().mela_batch_rank_null(self._plan, _ptr(d_in), _ptr(zt), _ptr(ranks),
+                                         1 if use_graph else 0, _stream(stream)))
+        return ranks, zt
+
+    def run_logical(self, d_logical, ranks=None, zt=None, use_graph: bool = True, stream=None):
+        if ranks is None:
+            ranks, zt = self.outputs(d_logical.device)
+        check(lib().mela_batch_rank_null_logical(self._plan, _ptr(d_logical), _ptr(zt), _ptr(ranks),
+                                                 1 if use_graph else 0, _stream(stream)))
+        return ranks, zt
+
+    def basis(self, zt_host, ranks_host, i):
+        """Packed basis of matrix i (nullity x ceil(n/64) uint64) from host copies."""
+        n = int(self.shapes[i, 1])
+        f = n - int(ranks_host[i])
+        wc = int(self.wc[i])
+        o = int(self.z_offsets[i])
+        return zt_host[o:o + f * wc].reshape(f, wc)
+
+    def close(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            lib().mela_batch_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
