@@ -1,25 +1,35 @@
 #!/usr/bin/env python
-"""Benchmark: GF(2) GEMM Tbitop/s at 32768^3 on B200.
+"""Benchmark: GF(2) GEMM Tbitop/s at 32768^3; batched rank+null mats/s.
 
-Workload (one step): C = A*B over GF(2) with A, B 32768 x 32768, iid
-Bernoulli(1/2) from seed 1, packed uint64 row-major, computed by the
-tcgen05 kind::i8 tensor-core form (operand preparation -- transpose of B and
-0/1 byte expansion -- plus the tensor-core kernel).  Bit-ops are counted as
-2*m*n*k (one AND and one XOR per term), the analogue of 2mnk FLOPs.
+Headline (value): C = A*B over GF(2) with A, B 32768 x 32768, iid
+Bernoulli(1/2) from seed 1, packed uint64 row-major, by the tcgen05 kind::i8
+tensor-core form (operand preparation -- transpose of B and 0/1 byte
+expansion -- plus the tensor-core kernel).  Bit-ops are counted as 2*m*n*k
+(one AND and one XOR per term), the analogue of 2mnk FLOPs.
 
   value  -- device-timed (CUDA events, max over ranks) with packed inputs
             resident in HBM; inputs are 256 MiB packed + 2 GiB of expanded
             operands per step, all larger than L2 (126 MB).
   e2e    -- the same product through the C ABI host entry point
-            mela_matmul_packed_host with pinned host buffers: the host->device
-            copy of A and B and the device->host copy of C are inside the
-            timed region of every step (host-timed around the blocking call).
-  roofline -- the tensor-core kernel alone, timed live with CUDA events on its
-            stream, against a dense INT8 peak measured in the same run
-            (cuBLASLt int8 GEMM through torch._int_mm).
+            mela_matmul_packed_host with pinned host buffers: host->device copy
+            of A and B and device->host copy of C inside every timed step
+            (host clock around the blocking call).
+  roofline -- the tensor-core kernel alone, CUDA events on its stream, against
+            dense INT8 measured in the same run (cuBLASLt int8 through
+            torch._int_mm).
   cpu_baseline -- the reference's own mela_matmul_gf2 (compiled from its
-            sources with its AVX512/OpenMP flags) on the host cores, on a
-            2048 x 32768 * 32768 x 2048 sub-block of the same product.
+            sources with its AVX512/OpenMP flags) on a 2048 x 32768 * 32768 x
+            2048 sub-block of the same product.
+  batched -- the second half of the metric: 20,000 parity-check matrices
+            (m uniform [64,1024], n = 2m +/- [0, m/4], six ones per row, seed 3)
+            ranked and null-spaced from their logical (MATLAB layout) form in
+            one persistent launch replayed as a CUDA graph, versus the plain
+            per-matrix path (one call sequence per matrix) on a sample.
+  dense_rank_null -- 16384 x 32768 rank-12000 matrix (seed 2): rank and null
+            space per elimination form, checked against the oracle's rank.
+  learned_dispatch -- a bounded sample of the mixed request stream (seed 4):
+            time of the installed cost model's choices vs the fixed rule vs the
+            exhaustive best.
 
 ``--impl reference`` times only the reference's CPU code (rank 0).
 """
@@ -39,13 +49,13 @@ sys.path.insert(0, ROOT)
 M = K = N = 32768
 SEED = 1
 BITOPS = 2.0 * M * N * K
+CPU_SAMPLE = (2048, 32768, 2048)  # rows of A, K, columns of B for the CPU legs
 
 
 def set_size(size: int) -> None:
     global M, K, N, BITOPS
     M = K = N = size
     BITOPS = 2.0 * M * N * K
-CPU_SAMPLE = (2048, 32768, 2048)  # rows of A, K, columns of B for the CPU legs
 
 
 # ------------------------------------------------------------------ clocks
@@ -104,40 +114,14 @@ class ClockSampler:
                     reasons.add(nm)
         sm.sort()
         med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
-
-
-# ------------------------------------------------------------------ distributed
-def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
-
-
-def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def max_over_ranks(ws, value: float) -> float:
-    if ws == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
 # ------------------------------------------------------------------ CPU legs
 def cpu_reference_sample(steps: int = 1):
-    """Time the reference gateway mela_matmul_gf2 (oracle/_ref) on the
-    CPU sample; returns (Tbitop/s, seconds per call, threads)."""
+    """Time the reference gateway mela_matmul_gf2 (oracle/_ref) on the CPU
+    sample; returns (Tbitop/s, seconds per call, threads, isa)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import oracle as O
     ms, ks, ns = CPU_SAMPLE
     A = O.unpack(O.rand_dense(SEED, 0, ms, ks), ms, ks)
@@ -193,7 +177,7 @@ def run_reference(args, ws, rank):
     return 0
 
 
-# ------------------------------------------------------------------ GPU leg
+# ------------------------------------------------------------------ GPU pieces
 def measure_int8_peak(torch):
     """Dense INT8 tensor throughput of cuBLASLt (torch._int_mm) at 8192^3."""
     n = 8192
@@ -214,8 +198,168 @@ def measure_int8_peak(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
+    """Batched rank+null of the parity-check batch from logical input."""
+    import numpy as np
+    from mex_linear_algebra_b200 import device as D, gen, _lib
+    from mex_linear_algebra_b200._lib import check, lib
+    shapes, offsets, buf = gen.ldpc_batch(count, seed)
+    plan = D.BatchPlan(shapes)
+    d_packed = torch.from_numpy(buf.view(np.int64)).cuda()
+    d_log = plan.unpack_logical(d_packed)
+    ranks, zt = plan.outputs()
+    for _ in range(3):
+        plan.run_logical(d_log, ranks, zt)
+    torch.cuda.synchronize()
+    reps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        plan.run_logical(d_log, ranks, zt)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    # plain per-matrix path: pack, RREF (plain form), null basis, one matrix at a time
+    L = lib()
+    s = torch.cuda.current_stream().cuda_stream
+    idx = np.linspace(0, count - 1, baseline_sample).astype(np.int64)
+    rk_host = ranks.cpu().numpy()
+    ok = True
+    t_base = 0.0
+    for i in idx:
+        m, n = int(shapes[i, 0]), int(shapes[i, 1])
+        wc = (n + 63) // 64
+        src = d_packed[offsets[i]:offsets[i] + m * wc].view(m, wc)
+        Mx = src.clone()
+        mn = min(m, n)
+        dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+        dpv = torch.empty(mn, dtype=torch.int64, device="cuda")
+        dpr = torch.empty(mn, dtype=torch.int64, device="cuda")
+        wsb = L.mela_elim_workspace_size(m, n)
+        wsp = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(L.mela_dev_rref(_lib.ELIM_PLAIN, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                              dpr.data_ptr(), wsp.data_ptr(), wsb, s))
+        r = int(dr.item())
+        f = n - r
+        Zt = torch.empty((max(f, 1), wc), dtype=torch.int64, device="cuda")
+        nwb = L.mela_null_workspace_size(n, r)
+        nws = torch.empty(max(nwb, 1), dtype=torch.uint8, device="cuda")
+        check(L.mela_dev_null_basis(Mx.data_ptr(), wc, m, n, r, dpv.data_ptr(), dpr.data_ptr(),
+                                    Zt.data_ptr(), wc, nws.data_ptr(), nwb, s))
+        torch.cuda.synchronize()
+        t_base += time.perf_counter() - t0
+        ok = ok and r == int(rk_host[i])
+        z0 = int(plan.z_offsets[i])
+        ok = ok and bool(torch.equal(Zt[:f].reshape(-1), zt[z0:z0 + f * wc]))
+    base_rate = baseline_sample / t_base
+    rate = count / (ms * 1e-3)
+    in_bytes = plan.logical_bytes
+    classes = plan.stats()
+    plan.close()
+    return {"metric": "batched rank+null mats/s", "value": round(rate, 1), "unit": "matrices/s",
+            "ms_per_batch": round(ms, 3), "matrices": count,
+            "input": f"logical (MATLAB layout), {in_bytes / 1e9:.2f} GB resident in HBM",
+            "engine": "one persistent launch replayed as a CUDA graph (warp / 128-thread group / CTA per matrix)",
+            "classes": classes,
+            "per_matrix_plain": {"value": round(base_rate, 1), "unit": "matrices/s",
+                                 "sample": f"{baseline_sample} matrices spread over the batch, "
+                                           "pack-free packed input, plain RREF + null basis per matrix, "
+                                           "host clock per matrix"},
+            "speedup_vs_per_matrix": round(rate / base_rate, 1), "results_match": ok}
+
+
+def bench_dense_rank(torch):
+    """Rank and null space of the 16384 x 32768 rank-12000 configuration."""
+    import numpy as np
+    from mex_linear_algebra_b200 import device as D, gen, _lib
+    from mex_linear_algebra_b200._lib import check, lib
+    m, r0, n = 16384, 12000, 32768
+    golden = None
+    gpath = os.path.join(ROOT, "tests", "golden", "dense_rank.json")
+    if os.path.exists(gpath):
+        golden = json.load(open(gpath))["rank"]
+    Ld = D.rand_dense(2, 0, m, r0)
+    Rd = D.rand_dense(2, 1, r0, n)
+    A = D.matmul(Ld, Rd, m, r0, n, variant="tc")
+    del Ld, Rd
+    for (i, a, b) in gen.replacement_triples(m, 164):
+        A[i] = A[a] ^ A[b]
+    L = lib()
+    s = torch.cuda.current_stream().cuda_stream
+    wc = n // 64
+    wsb = L.mela_elim_workspace_size(m, n)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    dpv = torch.empty(m, dtype=torch.int64, device="cuda")
+    dpr = torch.empty(m, dtype=torch.int64, device="cuda")
+    out = {"config": "A = L*R mod 2, L 16384x12000, R 12000x32768 (seed 2), 164 rows replaced by XORs "
+                     "of two others", "golden_rank": golden, "rank_ms": {}, "null_ms": {}}
+    ranks = set()
+    for form in ("m4ri", "m4ri_k4", "plain"):
+        v = _lib.ELIM_VARIANTS[form]
+        Mx = A.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        check(L.mela_dev_rank(v, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                              ws.data_ptr(), wsb, s))
+        e1.record()
+        e1.synchronize()
+        out["rank_ms"][form] = round(e0.elapsed_time(e1), 2)
+        ranks.add(int(dr.item()))
+    r = ranks.pop() if len(ranks) == 1 else None
+    out["rank"] = r
+    # null space through the blocked form: RREF + basis, then A * Z = 0 on the tensor cores
+    Mx = A.clone()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    check(L.mela_dev_rref(_lib.ELIM_M4RI, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                          dpr.data_ptr(), ws.data_ptr(), wsb, s))
+    e1.record()
+    e1.synchronize()
+    rr = int(dr.item())
+    f = n - rr
+    Zt = torch.empty((f, wc), dtype=torch.int64, device="cuda")
+    nwb = L.mela_null_workspace_size(n, rr)
+    nws = torch.empty(nwb, dtype=torch.uint8, device="cuda")
+    e1.record()
+    check(L.mela_dev_null_basis(Mx.data_ptr(), wc, m, n, rr, dpv.data_ptr(), dpr.data_ptr(),
+                                Zt.data_ptr(), wc, nws.data_ptr(), nwb, s))
+    e2.record()
+    e2.synchronize()
+    out["null_ms"]["m4ri_rref"] = round(e0.elapsed_time(e1), 2)
+    out["null_ms"]["basis"] = round(e1.elapsed_time(e2), 2)
+    Z = D.transpose(Zt, f, n)  # n x f
+    prod = D.matmul(A, Z, m, n, f, variant="tc")
+    out["nullity"] = f
+    out["A_times_Z_is_zero"] = bool(int(prod.abs().max().item()) == 0)
+    out["rank_matches_golden"] = (golden is None) or (r == golden and rr == golden)
+    del Zt, Z, prod, Mx, A, ws
+    torch.cuda.empty_cache()
+    return out
+
+
+def bench_dispatch(torch, count=200):
+    """Installed cost model vs fixed rule vs exhaustive best on a sample of
+    the mixed request stream (every variant timed live)."""
+    from mex_linear_algebra_b200 import autotune, costmodel
+    if not os.path.exists(costmodel.DEFAULT_MODEL):
+        return {"unavailable": "no trained cost model installed"}
+    params = costmodel.load()
+    recs = autotune.build_db(count, 200000, reps=2, max_cells=2e7)
+    rep = costmodel.evaluate(params, recs)
+    rep["sample"] = f"{len(recs)} requests of the mixed stream (seed 4) from request 200000, " \
+                    "each variant timed (median of 2 after a warm-up)"
+    rep["all_variants_bit_identical"] = all(r["agree"] for r in recs)
+    return rep
+
+
 def run_mela(args, ws, rank, local):
     import torch
+    from mex_linear_algebra_b200 import parallel
     torch.cuda.set_device(local)
     if ws > 1:
         import datetime
@@ -247,14 +391,14 @@ def run_mela(args, ws, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    barrier(ws)
+    parallel.barrier(ws)
 
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    barrier(ws)
+    parallel.barrier(ws)
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
@@ -265,30 +409,27 @@ def run_mela(args, ws, rank, local):
         e2.record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
-    barrier(ws)
+    parallel.barrier(ws)
     clk = clocks.stop()
-    total_ms = t_start.elapsed_time(t_end)
+    total_ms = parallel.max_over_ranks(ws, t_start.elapsed_time(t_end))
     kernel_ms = [e1.elapsed_time(e2) for (_, e1, e2) in evs]
-    total_ms = max_over_ranks(ws, total_ms)
     ms_step = total_ms / args.steps
     value = ws * BITOPS / (ms_step * 1e-3) / 1e12
     kern_avg = sum(kernel_ms) / len(kernel_ms)
 
     # correctness guard on the timed result: a block of rows against the plain form
-    ok = True
-    if rank == 0:
-        rows = 256
-        Cp = D.matmul(A[:rows], B, rows, K, N, variant="plain")
-        ok = bool(torch.equal(Cp, C[:rows]))
+    rows = 256
+    Cp = D.matmul(A[:rows], B, rows, K, N, variant="plain")
+    ok = bool(torch.equal(Cp, C[:rows]))
     flags = D.device_error_flags()
 
-    # the same product through the CUDA-core forms (one timed call each)
     forms = {"tc_ms": round(ms_step, 3)}
     if not args.quick:
         for name, var in (("plain", _lib.GEMM_PLAIN), ("m4ri", _lib.GEMM_M4RI)):
             wsv = D.matmul_workspace(var, M, K, N)
             wv = torch.empty(max(wsv, 1), dtype=torch.uint8, device="cuda")
             Cv = torch.empty_like(C)
+
             def run_form():
                 check(L.mela_dev_matmul(var, A.data_ptr(), wk, B.data_ptr(), wn, Cv.data_ptr(), wn,
                                         M, K, N, wv.data_ptr(), wsv, sptr))
@@ -309,10 +450,12 @@ def run_mela(args, ws, rank, local):
             print(json.dumps({"metric": "GF(2) GEMM Tbitop/s", "value": round(value, 3),
                               "unit": "Tbitop/s", "ms_per_step": round(ms_step, 4),
                               "kernel_ms": round(kern_avg, 4), "size": M, "result_check": ok}))
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return 0 if ok else 1
 
     # e2e through the C ABI with pinned host buffers
-    e2e = None
     del work
     torch.cuda.empty_cache()
     hA = torch.empty((M, wk), dtype=torch.int64, pin_memory=True)
@@ -320,7 +463,7 @@ def run_mela(args, ws, rank, local):
     hC = torch.empty((M, wn), dtype=torch.int64, pin_memory=True)
     hA.copy_(A)
     hB.copy_(B)
-    del A, B, C
+    del A, B, C, Cp
     torch.cuda.empty_cache()
 
     def e2e_step():
@@ -328,27 +471,34 @@ def run_mela(args, ws, rank, local):
                                         M, K, N, v))
 
     e2e_step()  # warm the stream-ordered pool
-    barrier(ws)
+    parallel.barrier(ws)
     e2e_steps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    dt_e2e = (time.perf_counter() - t0) / e2e_steps
-    dt_e2e = max_over_ranks(ws, dt_e2e)
+    dt_e2e = parallel.max_over_ranks(ws, (time.perf_counter() - t0) / e2e_steps)
     e2e = {"value": round(ws * BITOPS / dt_e2e / 1e12, 3), "unit": "Tbitop/s",
            "h2d_bytes_per_step": int(hA.numel() * 8 + hB.numel() * 8),
            "d2h_bytes_per_step": int(hC.numel() * 8), "ms_per_step": round(dt_e2e * 1e3, 3),
            "timing": "host clock around the blocking mela_matmul_packed_host call"}
     del hA, hB, hC
 
-    line = None
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        for name, fn in (("batched", bench_batched), ("dense_rank_null", bench_dense_rank),
+                         ("learned_dispatch", bench_dispatch)):
+            try:
+                extras[name] = fn(torch)
+            except Exception as e:  # reported, never silently dropped
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
     if rank == 0:
         peak = measure_int8_peak(torch)
         achieved = BITOPS / (kern_avg * 1e-3) / 1e12  # 2 int8 ops per MAC
-        cpu_rate, cpu_dt, threads, isa = (None, None, None, None)
+        cpu_rate, threads, isa = None, None, None
         try:
             os.environ.setdefault("OMP_DYNAMIC", "FALSE")
-            cpu_rate, cpu_dt, threads, isa = cpu_reference_sample(1)
+            cpu_rate, _, threads, isa = cpu_reference_sample(1)
         except Exception as e:  # reported, not fatal
             isa = f"unavailable: {e}"
         ms_, ks_, ns_ = CPU_SAMPLE
@@ -373,8 +523,9 @@ def run_mela(args, ws, rank, local):
             "roofline": {"bound": "tensor", "achieved": round(achieved, 1), "peak": round(peak, 1),
                          "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": None,
                          "kernel": "gemm_tc_kernel", "kernel_ms": round(kern_avg, 4),
-                         "peak_source": "dense INT8 measured in this run: cuBLASLt int8 GEMM "
-                                        "8192^3 via torch._int_mm, best of 10 (int8 ops as FLOPs)"},
+                         "peak_source": "dense INT8 measured in this run: cuBLASLt int8 GEMM 8192^3 "
+                                        "via torch._int_mm, best of 10 (int8 ops as FLOPs)",
+                         "frac_of_nominal_4500": round(achieved / 4500.0, 4)},
             "cpu_baseline": {"value": round(cpu_rate, 4) if cpu_rate else None, "unit": "Tbitop/s",
                              "cores": threads, "kind": "reference",
                              "sample": f"reference mela_matmul_gf2 ({isa}) on A {ms_}x{ks_} * B "
@@ -385,6 +536,7 @@ def run_mela(args, ws, rank, local):
             "clocks": clk,
             "device_error_flags": flags,
         }
+        line.update(extras)
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
@@ -400,12 +552,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mela", "reference"], default="mela")
     ap.add_argument("--size", type=int, default=32768,
-                    help="square problem size (32768 is the benchmark; smaller sizes are for profiling)")
+                    help="square product size (32768 is the benchmark; smaller sizes are for profiling)")
     ap.add_argument("--quick", action="store_true",
-                    help="device timing only: no e2e, CPU baseline, peak or form comparison")
+                    help="device timing only: no e2e, CPU baseline, peak, forms or extras")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched / dense-rank / dispatch sections")
     args = ap.parse_args()
     set_size(args.size)
-    ws, rank, local = dist_setup()
+    from mex_linear_algebra_b200 import parallel
+    ws, rank, local = parallel.world()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
     return run_mela(args, ws, rank, local)

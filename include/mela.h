@@ -76,7 +76,9 @@ typedef enum {
 typedef enum {
     MELA_ELIM_AUTO = 0,
     MELA_ELIM_PLAIN = 1,  /* per-pivot warp-ballot search + broadcast-XOR sweep */
-    MELA_ELIM_M4RI = 2    /* 64-column panels, Gray-code tables in shared memory */
+    MELA_ELIM_M4RI = 2,   /* 64-column panels, 8-bit Gray-code tables in shared memory */
+    MELA_ELIM_M4RI_K4 = 3, /* the same panels with 4-bit tables (M4RI k = 4) */
+    MELA_ELIM_FUSED = 4    /* the whole elimination by one CTA in one launch */
 } mela_elim_variant;
 
 /* ------------------------------------------------------------------ */
@@ -164,6 +166,11 @@ mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, const uint64
  * (seed, stream_id); bits past column n are zero. */
 mela_status mela_dev_rand_dense(uint64_t seed, uint64_t stream_id, int64_t m, int64_t n,
                                 uint64_t *d_out, int64_t ld, void *stream);
+
+/* Seeded Bernoulli(density) packed matrix: entry (i, j), e = i*n + j, is 1
+ * when 16-bit slice e%4 of stream word e/4 is below density*65536. */
+mela_status mela_dev_rand_bernoulli(uint64_t seed, uint64_t stream_id, int64_t m, int64_t n,
+                                    double density, uint64_t *d_out, int64_t ld, void *stream);
 
 /* Column-major logical (kind 0) or double (kind 1) m x n -> packed rows.
  * Replaces pack_rows_logical/pack_rows_double (src/mela_matmul_gf2.c:42-69)
@@ -261,6 +268,48 @@ mela_status mela_batch_rank_null(mela_batch_plan *plan, const uint64_t *d_in, ui
 mela_status mela_batch_rank_null_logical(mela_batch_plan *plan, const uint8_t *d_in,
                                          uint64_t *d_zt, int64_t *d_ranks, int32_t use_graph,
                                          void *stream);
+/* Every matrix of the batch from packed rows (in_offset layout) to its
+ * logical column-major form (the byte layout of the logical entry point). */
+mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_packed,
+                                      uint8_t *d_logical, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* learned dispatch: the cost model                                      */
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference.  A small MLP predicts the log2 running
+ * time (microseconds) of each of a request's kernel variants from its
+ * shape and density; the dispatcher takes the fastest prediction.  It only
+ * chooses how a result is computed: every variant returns the same bits.
+ * Parameters: one float array W1[8][32] b1[32] W2[32][32] b2[32] W3[32][4]
+ * b3[4].  Variant order per output: products (plain, m4ri, tc, -); rank and
+ * null space (plain, m4ri, m4ri_k4, fused). */
+#define MELA_MLP_IN 8
+#define MELA_MLP_H1 32
+#define MELA_MLP_H2 32
+#define MELA_MLP_OUT 4
+#define MELA_MLP_PARAMS 1476
+typedef enum { MELA_OP_RANK = 0, MELA_OP_NULL = 1, MELA_OP_MATMUL = 2 } mela_op;
+
+/* Y (N x 4) = network(X (N x 8)) on the device. */
+mela_status mela_mlp_forward(const float *d_params, const float *d_X, int64_t N, float *d_Y,
+                             void *stream);
+/* d_grad = gradient of the masked mean squared error between the network's
+ * outputs and targets T (N x 4, mask 1 where observed), scaled by inv_count
+ * = 1/(observed count); d_loss_sum (optional) = sum of squared errors. */
+mela_status mela_mlp_gradient(const float *d_params, const float *d_X, const float *d_T,
+                              const float *d_mask, int64_t N, float inv_count, float *d_grad,
+                              float *d_loss_sum, void *stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8); step counts from 1. */
+mela_status mela_mlp_adam_step(float *d_params, const float *d_grad, float *d_m1, float *d_m2,
+                               int64_t step, float lr, void *stream);
+/* Install (or, with NULL, remove) the dispatch model from host memory. */
+mela_status mela_costmodel_load(const float *h_params);
+/* Variant index (0..3) the installed model picks, or -1 when none is
+ * installed (the fixed rule is used then). */
+int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density);
+/* The 8 input features of a request. */
+void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
+                             float *x);
 
 /* ------------------------------------------------------------------ */
 /* allocation-free product                                              */

@@ -23,9 +23,15 @@ GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc"
 
 # mela_function (gateway ids)
 FN_MATMUL_GF2, FN_MATMUL_M4RI, FN_RANK_GF2, FN_RANK_M4RI, FN_NULL_GF2, FN_NULL_M4RI = range(6)
+# mela_op and the cost model's shape
+OP_RANK, OP_NULL, OP_MATMUL = 0, 1, 2
+MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 4, 1476
+# variant index (model output) -> variant code, per op
+OP_VARIANTS = {OP_MATMUL: (1, 2, 3), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
 # mela_elim_variant
-ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI = 0, 1, 2
-ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI}
+ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI, ELIM_M4RI_K4, ELIM_FUSED = 0, 1, 2, 3, 4
+ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI, "m4ri_k4": ELIM_M4RI_K4,
+                 "fused": ELIM_FUSED}
 
 
 class GatewayError(C.Structure):
@@ -63,6 +69,7 @@ SIGNATURES = {
                                C.POINTER(GatewayError)]),
     "mela_matmul_packed_host": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i32]),
     "mela_dev_rand_dense": (_st, [_u64, _u64, _i64, _i64, _vp, _i64, _vp]),
+    "mela_dev_rand_bernoulli": (_st, [_u64, _u64, _i64, _i64, C.c_double, _vp, _i64, _vp]),
     "mela_dev_pack": (_st, [_i32, _i64, _i64, _vp, _vp, _i64, _vp]),
     "mela_dev_unpack": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
     "mela_dev_transpose": (_st, [_vp, _i64, _i64, _i64, _vp, _i64, _vp]),
@@ -81,6 +88,13 @@ SIGNATURES = {
     "mela_batch_plan_stats": (_st, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "mela_batch_rank_null": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
     "mela_batch_rank_null_logical": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "mela_batch_unpack_logical": (_st, [_vp, _vp, _vp, _vp]),
+    "mela_mlp_forward": (_st, [_vp, _vp, _i64, _vp, _vp]),
+    "mela_mlp_gradient": (_st, [_vp, _vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp]),
+    "mela_mlp_adam_step": (_st, [_vp, _vp, _vp, _vp, _i64, C.c_float, _vp]),
+    "mela_costmodel_load": (_st, [_vp]),
+    "mela_costmodel_choose": (_i32, [_i32, _i64, _i64, _i64, C.c_double]),
+    "mela_costmodel_features": (None, [_i32, _i64, _i64, _i64, C.c_double, _vp]),
     "mela_static_scratch_bytes": (_sz, []),
     "mela_dev_matmul_plain_static": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp]),
 }

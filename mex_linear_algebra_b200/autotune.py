@@ -1,0 +1,168 @@
+"""Exhaustive autotuner: time every kernel variant of a request on the GPU.
+
+For each request (op, m, n, p, density) the inputs are generated on the
+device from the seeded Bernoulli generator, every variant runs once to warm
+up and ``reps`` times under CUDA events, and the median is recorded in
+microseconds.  The variants' results are compared with each other (they must
+be bit-identical) and the record says so.  Records form the timing database
+the cost model is trained on, and the exhaustive best time of each request is
+the judge of the model's regret.
+
+    python -m mex_linear_algebra_b200.autotune --count 600 --offset 100000 --out db.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import _lib, gen
+from ._lib import check, lib
+from .costmodel import VARIANT_NAMES
+
+SEED = 4
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _bernoulli(torch, seed, stream_id, m, n, density):
+    wc = (n + 63) // 64
+    t = torch.empty((max(m, 1), max(wc, 1)), dtype=torch.int64, device="cuda")
+    check(lib().mela_dev_rand_bernoulli(seed, stream_id, m, n, density, t.data_ptr(), t.shape[1],
+                                        torch.cuda.current_stream().cuda_stream))
+    return t
+
+
+def time_matmul(torch, m, k, n, density, stream_id, reps=3):
+    L = lib()
+    s = torch.cuda.current_stream().cuda_stream
+    A = _bernoulli(torch, SEED, 2 * stream_id, m, k, density)
+    B = _bernoulli(torch, SEED, 2 * stream_id + 1, k, n, density)
+    wn = (n + 63) // 64
+    times, outs = {}, {}
+    for v, name in zip((_lib.GEMM_PLAIN, _lib.GEMM_M4RI, _lib.GEMM_TC), VARIANT_NAMES["matmul"]):
+        wsb = L.mela_matmul_workspace_size(v, m, k, n)
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+        C_ = torch.empty((m, wn), dtype=torch.int64, device="cuda")
+
+        def run():
+            check(L.mela_dev_matmul(v, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
+                                    C_.data_ptr(), wn, m, k, n, ws.data_ptr(), wsb, s))
+        run()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = _events(torch)
+            e0.record()
+            run()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e3)
+        times[name] = float(np.median(ts))
+        outs[name] = C_
+    agree = all(torch.equal(outs[x], outs["plain"]) for x in outs)
+    return times, agree
+
+
+def time_elim(torch, op, m, n, density, stream_id, reps=3):
+    L = lib()
+    s = torch.cuda.current_stream().cuda_stream
+    A0 = _bernoulli(torch, SEED, 2 * stream_id, m, n, density)
+    wc = (n + 63) // 64
+    mn = max(min(m, n), 1)
+    wsb = L.mela_elim_workspace_size(m, n)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    rank = torch.zeros(1, dtype=torch.int64, device="cuda")
+    piv = torch.empty(mn, dtype=torch.int64, device="cuda")
+    prow = torch.empty(mn, dtype=torch.int64, device="cuda")
+    times, results = {}, {}
+    for v, name in zip((_lib.ELIM_PLAIN, _lib.ELIM_M4RI, _lib.ELIM_M4RI_K4, _lib.ELIM_FUSED),
+                       VARIANT_NAMES[op]):
+        ts = []
+        for rep in range(reps + 1):
+            M = A0.clone()
+            torch.cuda.synchronize()
+            e0, e1 = _events(torch)
+            e0.record()
+            fn = L.mela_dev_rref if op == "null" else L.mela_dev_rank
+            check(fn(v, M.data_ptr(), wc, m, n, rank.data_ptr(), piv.data_ptr(), prow.data_ptr(),
+                     ws.data_ptr(), wsb, s))
+            e1.record()
+            e1.synchronize()
+            t = e0.elapsed_time(e1) * 1e3
+            r = int(rank.item())
+            res = (r,)
+            if op == "null":
+                f = n - r
+                Zt = torch.empty((max(f, 1), wc), dtype=torch.int64, device="cuda")
+                nwb = L.mela_null_workspace_size(n, r)
+                nws = torch.empty(max(nwb, 1), dtype=torch.uint8, device="cuda")
+                e2, e3 = _events(torch)
+                e2.record()
+                check(L.mela_dev_null_basis(M.data_ptr(), wc, m, n, r, piv.data_ptr(), prow.data_ptr(),
+                                            Zt.data_ptr(), wc, nws.data_ptr(), nwb, s))
+                e3.record()
+                e3.synchronize()
+                t += e2.elapsed_time(e3) * 1e3
+                res = (r, Zt[:f].clone())
+            if rep > 0:
+                ts.append(t)
+        times[name] = float(np.median(ts))
+        results[name] = res
+    base = results["plain"]
+    agree = True
+    for x in results.values():
+        if x[0] != base[0]:
+            agree = False
+        elif op == "null" and not torch.equal(x[1], base[1]):
+            agree = False
+    return times, agree
+
+
+def time_request(req, reps=3):
+    import torch
+    op, m, n, p, d, sid = req["op"], req["m"], req["n"], req.get("p", 0), req["density"], req["stream"]
+    if op == "matmul":
+        times, agree = time_matmul(torch, m, n, p, d, sid, reps)
+    else:
+        times, agree = time_elim(torch, op, m, n, d, sid, reps)
+    out = dict(req)
+    out["times_us"] = times
+    out["agree"] = bool(agree)
+    return out
+
+
+def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 4e7, verbose: bool = False):
+    """Time `count` requests of the mixed stream starting at request `offset`.
+    Requests whose matrices exceed `max_cells` bits are skipped (bounded run)."""
+    reqs = gen.mixed_stream(offset + count, SEED)[offset:]
+    db = []
+    t0 = time.time()
+    for i, r in enumerate(reqs):
+        cells = r["m"] * r["n"] + (r["n"] * r["p"] if r["op"] == "matmul" else 0)
+        if cells > max_cells:
+            continue
+        db.append(time_request(r, reps))
+        if verbose and (i + 1) % 50 == 0:
+            print(f"{i + 1}/{count} timed, {time.time() - t0:.1f}s", flush=True)
+    return db
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", type=int, default=600)
+    ap.add_argument("--offset", type=int, default=100000)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--out", default="autotune_db.json")
+    a = ap.parse_args()
+    db = build_db(a.count, a.offset, a.reps, verbose=True)
+    with open(a.out, "w") as f:
+        json.dump(db, f)
+    print(f"{len(db)} records -> {a.out}; all variants agree: {all(r['agree'] for r in db)}")
+
+
+if __name__ == "__main__":
+    main()

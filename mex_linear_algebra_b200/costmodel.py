@@ -1,0 +1,165 @@
+"""The learned cost model: training on the GPU, saving, loading, choosing.
+
+Training runs entirely in the library's kernels (mela_mlp_gradient +
+mela_mlp_adam_step, full-batch Adam); torch only holds the buffers.  The
+model predicts log2(microseconds) for each of a request's variants;
+``choose`` returns the variant with the smallest prediction, and
+``install`` hands the weights to the library's dispatcher.  Without an
+installed model the library uses its fixed rule.
+
+Timing databases come from :mod:`mex_linear_algebra_b200.autotune`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_MODEL = os.path.join(PKG, "costmodel.json")
+OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL}
+VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc"), "rank": ("plain", "m4ri", "m4ri_k4", "fused"),
+                 "null": ("plain", "m4ri", "m4ri_k4", "fused")}
+
+
+def features(op: str, m: int, n: int, p: int, density: float) -> np.ndarray:
+    x = (C.c_float * _lib.MLP_IN)()
+    lib().mela_costmodel_features(OPS[op], int(m), int(n), int(p), float(density), x)
+    return np.array(list(x), dtype=np.float32)
+
+
+def dataset(records):
+    """Records (autotune DB rows) -> X (N x 8), T (N x 4 log2 us), mask (N x 4)."""
+    X = np.stack([features(r["op"], r["m"], r["n"], r.get("p", 0), r["density"]) for r in records])
+    T = np.zeros((len(records), _lib.MLP_OUT), dtype=np.float32)
+    Mk = np.zeros_like(T)
+    for i, r in enumerate(records):
+        for v, name in enumerate(VARIANT_NAMES[r["op"]]):
+            t = r["times_us"].get(name)
+            if t is not None and t > 0:
+                T[i, v] = np.log2(t)
+                Mk[i, v] = 1.0
+    return X, T, Mk
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fan_in, fan_out in ((_lib.MLP_IN, _lib.MLP_H1), (_lib.MLP_H1, _lib.MLP_H2), (_lib.MLP_H2, _lib.MLP_OUT)):
+        parts.append(rng.normal(0, np.sqrt(2.0 / fan_in), size=(fan_in, fan_out)).ravel())
+        parts.append(np.zeros(fan_out))
+    p = np.concatenate(parts).astype(np.float32)
+    assert p.size == _lib.MLP_PARAMS
+    return p
+
+
+def train(records, steps: int = 3000, lr: float = 3e-3, seed: int = 0, log_every: int = 0):
+    """Full-batch Adam on the GPU.  Returns (params float32, final loss)."""
+    import torch
+    X, T, Mk = dataset(records)
+    dev = torch.device("cuda")
+    dX = torch.from_numpy(X).to(dev)
+    dT = torch.from_numpy(T).to(dev)
+    dM = torch.from_numpy(Mk).to(dev)
+    P = torch.from_numpy(init_params(seed)).to(dev)
+    G = torch.zeros_like(P)
+    m1 = torch.zeros_like(P)
+    m2 = torch.zeros_like(P)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    inv = 1.0 / max(float(Mk.sum()), 1.0)
+    s = torch.cuda.current_stream().cuda_stream
+    L = lib()
+    last = None
+    for step in range(1, steps + 1):
+        check(L.mela_mlp_gradient(P.data_ptr(), dX.data_ptr(), dT.data_ptr(), dM.data_ptr(), len(X),
+                                  inv, G.data_ptr(), loss.data_ptr(), s))
+        check(L.mela_mlp_adam_step(P.data_ptr(), G.data_ptr(), m1.data_ptr(), m2.data_ptr(), step, lr, s))
+        if log_every and step % log_every == 0:
+            print(f"step {step} loss {loss.item() * inv:.4f}")
+    last = float(loss.item()) * inv
+    return P.cpu().numpy(), last
+
+
+def predict(params: np.ndarray, X: np.ndarray) -> np.ndarray:
+    import torch
+    dP = torch.from_numpy(np.ascontiguousarray(params, dtype=np.float32)).cuda()
+    dX = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).cuda()
+    dY = torch.empty((len(X), _lib.MLP_OUT), dtype=torch.float32, device="cuda")
+    check(lib().mela_mlp_forward(dP.data_ptr(), dX.data_ptr(), len(X), dY.data_ptr(),
+                                 torch.cuda.current_stream().cuda_stream))
+    return dY.cpu().numpy()
+
+
+def save(params: np.ndarray, path: str = DEFAULT_MODEL, meta: dict | None = None):
+    with open(path, "w") as f:
+        json.dump({"params": [float(x) for x in params], "meta": meta or {}}, f)
+
+
+def load(path: str = DEFAULT_MODEL) -> np.ndarray:
+    with open(path) as f:
+        return np.array(json.load(f)["params"], dtype=np.float32)
+
+
+def install(params: np.ndarray | None):
+    """Give the weights to the library's dispatcher (None removes them)."""
+    if params is None:
+        check(lib().mela_costmodel_load(None))
+        return
+    buf = np.ascontiguousarray(params, dtype=np.float32)
+    if buf.size != _lib.MLP_PARAMS:
+        raise ValueError(f"cost model has {buf.size} parameters, the library expects {_lib.MLP_PARAMS}")
+    check(lib().mela_costmodel_load(buf.ctypes.data))
+
+
+def choose(op: str, m: int, n: int, p: int, density: float) -> str:
+    """Variant the installed model picks (name); the fixed rule without one."""
+    v = lib().mela_costmodel_choose(OPS[op], int(m), int(n), int(p), float(density))
+    if v < 0:
+        return heuristic(op, m, n, p, density)
+    return VARIANT_NAMES[op][v]
+
+
+def heuristic(op: str, m: int, n: int, p: int, density: float) -> str:
+    """The library's fixed rule (what dispatch does without a model)."""
+    if op == "matmul":
+        return "tc" if (m >= 1024 and n >= 1024 and p >= 1024) else "plain"
+    return "m4ri"
+
+
+def evaluate(params: np.ndarray, records):
+    """Measured cost of the model's choices vs the exhaustive best and vs the
+    fixed rule, on records with every variant timed: totals (dominated by the
+    largest requests) and per-request means of time/best - 1."""
+    X, T, Mk = dataset(records)
+    Y = predict(params, X) if len(X) else np.zeros((0, _lib.MLP_OUT))
+    tot_best = tot_model = tot_rule = 0.0
+    reg_model, reg_rule = [], []
+    agree = used = 0
+    for i, r in enumerate(records):
+        names = VARIANT_NAMES[r["op"]]
+        times = [r["times_us"].get(nm) for nm in names]
+        if any(t is None for t in times):
+            continue
+        used += 1
+        best = min(times)
+        pred = int(np.argmin(np.where(Mk[i, :len(names)] > 0, Y[i, :len(names)], np.inf)))
+        rule = names.index(heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"]))
+        tot_best += best
+        tot_model += times[pred]
+        tot_rule += times[rule]
+        reg_model.append(times[pred] / best - 1.0)
+        reg_rule.append(times[rule] / best - 1.0)
+        agree += int(times[pred] == best)
+    return {"records": used, "total_best_us": tot_best, "total_model_us": tot_model,
+            "total_rule_us": tot_rule,
+            "regret": tot_model / tot_best - 1.0 if tot_best else 0.0,
+            "rule_regret": tot_rule / tot_best - 1.0 if tot_best else 0.0,
+            "speedup_vs_rule": tot_rule / tot_model if tot_model else 0.0,
+            "mean_request_regret": float(np.mean(reg_model)) if reg_model else 0.0,
+            "rule_mean_request_regret": float(np.mean(reg_rule)) if reg_rule else 0.0,
+            "picked_best_frac": agree / max(used, 1)}

@@ -152,8 +152,11 @@ struct GemmPlan {
 
 int choose_gemm_variant(i64 m, i64 k, i64 n)
 {
-    // Tensor cores pay off once every dimension spans a few tiles; below that
-    // the expansion to bytes dominates.  (The autotuner refines this table.)
+    // the learned cost model when one is installed (dense input assumed)
+    const int c = costmodel_choose(MELA_OP_MATMUL, (double)m, (double)k, (double)n, 0.5);
+    if (c >= 0) return c == 0 ? MELA_GEMM_PLAIN : (c == 1 ? MELA_GEMM_M4RI : MELA_GEMM_TC);
+    // fixed rule: tensor cores pay off once every dimension spans a few
+    // tiles; below that the expansion to bytes dominates
     if (m >= 1024 && n >= 1024 && k >= 1024) return MELA_GEMM_TC;
     return MELA_GEMM_PLAIN;
 }

@@ -40,6 +40,14 @@ struct BatchDevItem {
     long long in_off, z_off;
 };
 
+// Outputs of the single-matrix ("fused") mode: instead of a null basis, the
+// RREF rows are written back over the caller's matrix, with the pivot lists.
+struct FusedOut {
+    u64 *M;
+    long long ldm;
+    long long *rank, *piv, *prow;
+};
+
 namespace {
 constexpr int kThreads = 512;
 constexpr int kMidGroup = 128;
@@ -80,7 +88,7 @@ __device__ __forceinline__ int ctz64b(u64 x) { return __ffsll((long long)x) - 1;
 template <int G>
 __device__ void process_matrix(const BatchDevItem &it, const u64 *__restrict__ in, u64 *__restrict__ zt,
                                long long *ranks, int item, unsigned char *region, u64 *gmat, int gtid,
-                               int bar_id)
+                               int bar_id, const FusedOut *fo = nullptr)
 {
     const int m = it.m, n = it.n, wc = (n + 63) >> 6, mn = m < n ? m : n;
     const bool in_smem = it.flags & 1;
@@ -145,6 +153,20 @@ __device__ void process_matrix(const BatchDevItem &it, const u64 *__restrict__ i
         }
         search(c + 1);
         group_sync(G, bar_id);
+    }
+    if (fo) {
+        // single-matrix mode: RREF rows back to the caller, pivot lists, rank
+        for (long long e = gtid; e < (long long)m * wc; e += G) {
+            const int rr = (int)(e / wc), x = (int)(e - (long long)rr * wc);
+            fo->M[(long long)rr * fo->ldm + x] = A[(size_t)rr * ld + x];
+        }
+        for (int t = gtid; t < r; t += G) {
+            fo->piv[t] = piv[t];
+            fo->prow[t] = prow[t];
+        }
+        if (gtid == 0) *fo->rank = r;
+        group_sync(G, bar_id);
+        return;
     }
     if (gtid == 0) ranks[item] = r;
 
@@ -268,7 +290,7 @@ __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dl
 //    otherwise -- three 32x32 ballot transposes, no per-bit gathers.
 __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restrict__ in,
                                     u64 *__restrict__ zt, long long *ranks, int item,
-                                    unsigned char *smem_raw, u64 *g)
+                                    unsigned char *smem_raw, u64 *g, const FusedOut *fo = nullptr)
 {
     BigSmem &S = *reinterpret_cast<BigSmem *>(smem_raw);
     const int m = it.m, n = it.n, wc = (n + 63) >> 6, mn = m < n ? m : n;
@@ -444,6 +466,19 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         r += p;
         __syncthreads();
     }
+    if (fo) {
+        for (long long e = tid; e < (long long)m * wc; e += kThreads) {
+            const int rr = (int)(e / wc), x = (int)(e - (long long)rr * wc);
+            fo->M[(long long)rr * fo->ldm + x] = A[e];
+        }
+        for (int t = tid; t < r; t += kThreads) {
+            fo->piv[t] = piv[t];
+            fo->prow[t] = prow[t];
+        }
+        if (tid == 0) *fo->rank = r;
+        __syncthreads();
+        return;
+    }
     if (tid == 0) ranks[item] = r;
 
     // ---- null basis
@@ -580,6 +615,85 @@ __global__ void batch_pack_kernel(const BatchDevItem *__restrict__ items, const 
     u64 word = 0;
     for (int j = 0; j < cols; ++j) word |= (u64)(p[(long long)j * it.m] != 0) << j;
     out[it.in_off + (long long)row * wc + w] = word;
+}
+
+// packed rows -> logical column-major inputs, for every matrix of the batch
+__global__ void batch_unpack_kernel(const BatchDevItem *__restrict__ items, const long long *byte_off,
+                                    const long long *tile_start, int count, const u64 *__restrict__ in,
+                                    unsigned char *__restrict__ out)
+{
+    const long long b = blockIdx.x;
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const BatchDevItem it = items[lo];
+    const long long tile = b - tile_start[lo];
+    const int wc = (it.n + 63) >> 6, wg = (wc + 7) / 8;
+    const int rt = (int)(tile / wg), wt = (int)(tile % wg);
+    const int lane = threadIdx.x & 31, w8 = threadIdx.x >> 5;
+    const int row = rt * 32 + lane, w = wt * 8 + w8;
+    if (row >= it.m || w >= wc) return;
+    const u64 word = in[it.in_off + (long long)row * wc + w];
+    unsigned char *p = out + byte_off[lo] + row + (long long)w * 64 * it.m;
+    const int cols = (it.n - w * 64) < 64 ? (it.n - w * 64) : 64;
+    for (int j = 0; j < cols; ++j) p[(long long)j * it.m] = (unsigned char)((word >> j) & 1);
+}
+
+// ---------------------------------------------------------------- single matrix
+// RREF of one matrix by one CTA in one launch: in shared memory by the
+// column-by-column engine when it fits, else by the blocked engine over
+// global scratch.  Reads the packed matrix M (row pitch ldm, any pitch >=
+// ceil(n/64)) and writes the RREF rows back over it.
+__global__ void __launch_bounds__(kThreads, 1)
+fused_elim_kernel(BatchDevItem it, const u64 *__restrict__ in_compact, FusedOut fo, u64 *scratch)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (it.flags & 1)
+        process_matrix<kThreads>(it, in_compact, nullptr, nullptr, 0, smem, nullptr, threadIdx.x, 0, &fo);
+    else
+        process_big_blocked(it, in_compact, nullptr, nullptr, 0, smem, scratch, &fo);
+}
+
+size_t fused_workspace(i64 m, i64 n)
+{
+    const i64 wc = words_of(n);
+    // compact copy of the input (pitch ceil(n/64)) + big-engine scratch
+    return (size_t)(m * wc + big_scratch_words(m, n)) * 8;
+}
+
+mela_status launch_fused_elim(u64 *M, i64 ld, i64 m, i64 n, long long *d_rank, long long *d_piv,
+                              long long *d_prow, void *ws, size_t ws_bytes, cudaStream_t s)
+{
+    if (m > INT_MAX / 2 || n > INT_MAX / 2) {
+        set_error("fused elimination: matrix too large");
+        return MELA_ERR_UNSUPPORTED;
+    }
+    const size_t need = fused_workspace(m, n);
+    if (ws_bytes < need || !ws) {
+        set_error("fused elimination workspace of %zu bytes needed, %zu given", need, ws_bytes);
+        return MELA_ERR_INVALID;
+    }
+    const i64 wc = words_of(n);
+    u64 *compact = (u64 *)ws;
+    u64 *scratch = compact + m * wc;
+    MELA_CUDA_TRY(cudaMemcpy2DAsync(compact, (size_t)wc * 8, M, (size_t)ld * 8, (size_t)wc * 8, (size_t)m,
+                                    cudaMemcpyDeviceToDevice, s));
+    BatchDevItem it{};
+    it.m = (int)m;
+    it.n = (int)n;
+    it.in_off = 0;
+    it.z_off = 0;
+    const size_t aux = aux_bytes((int)m, (int)n);
+    const size_t mat = (size_t)m * smem_ld((int)n) * 8;
+    it.flags = (aux + mat <= (size_t)kSmemTotal) ? 1 : 0;
+    FusedOut fo{M, ld, d_rank, d_piv, d_prow};
+    MELA_CUDA_TRY(cudaFuncSetAttribute(fused_elim_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kSmemTotal));
+    fused_elim_kernel<<<1, kThreads, kSmemTotal, s>>>(it, compact, fo, scratch);
+    MELA_LAUNCH_CHECK("fused_elim_kernel");
+    return MELA_OK;
 }
 
 // ---------------------------------------------------------------- host side
@@ -840,6 +954,22 @@ extern "C" mela_status mela_batch_rank_null(mela_batch_plan *plan, const uint64_
         return MELA_ERR_INVALID;
     }
     return run(plan->impl, d_in, 0, (u64 *)d_zt, (long long *)d_ranks, (cudaStream_t)stream, use_graph);
+}
+
+extern "C" mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_packed,
+                                                 uint8_t *d_logical, void *stream)
+{
+    if (!plan || (plan->impl->count && (!d_packed || !d_logical))) {
+        set_error("mela_batch_unpack_logical: null argument");
+        return MELA_ERR_INVALID;
+    }
+    BatchPlanImpl *P = plan->impl;
+    if (P->count && P->pack_tiles) {
+        batch_unpack_kernel<<<(unsigned)P->pack_tiles, 256, 0, (cudaStream_t)stream>>>(
+            P->d_items, P->d_byte_off, P->d_tile_start, P->count, (const u64 *)d_packed, d_logical);
+        MELA_LAUNCH_CHECK("batch_unpack_kernel");
+    }
+    return MELA_OK;
 }
 
 extern "C" mela_status mela_batch_rank_null_logical(mela_batch_plan *plan, const uint8_t *d_in,

@@ -229,6 +229,63 @@ panel_update_kernel(u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const Pan
     }
 }
 
+// 4-bit variant: 16 tables of the 16 combinations of 4 R rows (k = 4); a row
+// looks up 16 entries per word instead of 8, but a table costs 16x less to
+// build -- the better choice when few rows share a panel.
+namespace {
+constexpr int UPD4_TW = 8;
+}
+__global__ void __launch_bounds__(256)
+panel_update_k4_kernel(u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const PanelState *ps,
+                       const u64 *__restrict__ Rbuf, const unsigned char *state, const int *stamp,
+                       int panel, int rref, const u64 *__restrict__ ysnap)
+{
+    __shared__ u64 T[16][16][UPD4_TW];
+    const int p = ps->p;
+    if (p == 0) return;
+    const u64 pm = ps->pivmask;
+    const i64 w0 = w + (i64)blockIdx.x * UPD4_TW;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 16 * 5 * UPD4_TW; e += 256) {
+        const int t = e % UPD4_TW, gh = e / UPD4_TW, g = gh / 5, h = gh % 5;
+        const i64 word = w0 + t;
+        if (h == 4) {
+            T[g][0][t] = 0;
+            continue;
+        }
+        const int b = 4 * g + h;
+        u64 v = 0;
+        if (((pm >> b) & 1) && word < wc) {
+            const int k = __popcll(pm & ((1ull << b) - 1));
+            v = Rbuf[(i64)k * wc + word];
+        }
+        T[g][1 << h][t] = v;
+    }
+    __syncthreads();
+    for (int h = 1; h < 4; ++h) {
+        const int cnt = (1 << h) - 1;
+        for (int e = tid; e < 16 * cnt * UPD4_TW; e += 256) {
+            const int t = e % UPD4_TW, rest = e / UPD4_TW, g = rest / cnt, v = (1 << h) + 1 + rest % cnt;
+            T[g][v][t] = T[g][v - (1 << h)][t] ^ T[g][1 << h][t];
+        }
+        __syncthreads();
+    }
+    const i64 row0 = (i64)blockIdx.y * UPD_RT;
+    const int t = tid % UPD4_TW;
+    const i64 word = w0 + t;
+    for (int rr = tid / UPD4_TW; rr < UPD_RT; rr += 256 / UPD4_TW) {
+        const i64 j = row0 + rr;
+        if (j >= m) break;
+        if (rref ? (stamp[j] == panel) : (state[j] == 0)) continue;
+        const u64 y = ysnap[j] & pm;
+        if (!y || word >= wc) continue;
+        u64 acc = 0;
+#pragma unroll
+        for (int g = 0; g < 16; ++g) acc ^= T[g][(y >> (4 * g)) & 15][t];
+        M[j * ld + word] ^= acc;
+    }
+}
+
 // ---------------------------------------------------------------- plain form
 struct GridBar {
     unsigned count;
@@ -480,20 +537,25 @@ ElimLayout elim_layout(i64 m, i64 n)
     return L;
 }
 
-size_t elim_workspace(i64 m, i64 n) { return elim_layout(m, n).total; }
-
-int choose_elim_variant(i64 m, i64 n)
+size_t elim_workspace(i64 m, i64 n)
 {
-    (void)m;
-    (void)n;
-    return MELA_ELIM_M4RI;
+    const size_t a = elim_layout(m, n).total, b = fused_workspace(m, n);
+    return a > b ? a : b;
+}
+
+int choose_elim_variant(i64 m, i64 n, int rref)
+{
+    const int c = costmodel_choose(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0, 0.5);
+    static const int order[4] = {MELA_ELIM_PLAIN, MELA_ELIM_M4RI, MELA_ELIM_M4RI_K4, MELA_ELIM_FUSED};
+    if (c >= 0 && c < 4) return order[c];
+    return MELA_ELIM_M4RI;  // fixed rule: the blocked form
 }
 
 mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank,
                         long long *d_piv, long long *d_prow, void *ws, size_t ws_bytes,
                         cudaStream_t s)
 {
-    if (variant == MELA_ELIM_AUTO) variant = choose_elim_variant(m, n);
+    if (variant == MELA_ELIM_AUTO) variant = choose_elim_variant(m, n, rref);
     if (m == 0 || n == 0) {
         MELA_CUDA_TRY(cudaMemsetAsync(d_rank, 0, sizeof(long long), s));
         return MELA_OK;
@@ -502,9 +564,11 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
         set_error("elimination: more than 2^31-2 rows");
         return MELA_ERR_UNSUPPORTED;
     }
+    if (variant == MELA_ELIM_FUSED)
+        return launch_fused_elim(M, ld, m, n, d_rank, d_piv, d_prow, ws, ws_bytes, s);
     ElimLayout L = elim_layout(m, n);
     if (ws_bytes < L.total || !ws) {
-        set_error("elimination workspace of %zu bytes needed, %zu given", L.total, ws_bytes);
+        set_error("elimination workspace of %zu bytes needed, %zu given", elim_workspace(m, n), ws_bytes);
         return MELA_ERR_INVALID;
     }
     unsigned char *w = (unsigned char *)ws;
@@ -548,7 +612,7 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
         MELA_LAUNCH_CHECK("ge_plain_kernel");
         return MELA_OK;
     }
-    if (variant != MELA_ELIM_M4RI) {
+    if (variant != MELA_ELIM_M4RI && variant != MELA_ELIM_M4RI_K4) {
         set_error("unknown elimination variant %d", variant);
         return MELA_ERR_INVALID;
     }
@@ -570,9 +634,13 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
                                                        d_piv, d_prow, ysnap);
         const i64 rem = wc - pw;
         panel_rows_kernel<<<(unsigned)((rem + 31) / 32), 256, 0, s>>>(M, ld, wc, pw, ps, rbuf);
-        panel_update_kernel<<<dim3((unsigned)((rem + UPD_TW - 1) / UPD_TW), (unsigned)rtiles), 256,
-                              upd_smem, s>>>(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref,
-                                             ysnap);
+        if (variant == MELA_ELIM_M4RI_K4)
+            panel_update_k4_kernel<<<dim3((unsigned)((rem + UPD4_TW - 1) / UPD4_TW), (unsigned)rtiles), 256, 0,
+                                     s>>>(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref, ysnap);
+        else
+            panel_update_kernel<<<dim3((unsigned)((rem + UPD_TW - 1) / UPD_TW), (unsigned)rtiles), 256,
+                                  upd_smem, s>>>(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref,
+                                                 ysnap);
     }
     MELA_LAUNCH_CHECK("panel elimination");
     MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &ps->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));

@@ -26,6 +26,9 @@ mela_status finish(cudaStream_t s);
 i64 even_words(i64 bits);
 
 int choose_gemm_variant(i64 m, i64 k, i64 n);
+// Learned cost model: variant index 0..2 for the request, or -1 without a model.
+int costmodel_choose(int op, double m, double n, double p, double density);
+void costmodel_features(int op, double m, double n, double p, double density, float *x);
 size_t gemm_workspace(int variant, i64 m, i64 k, i64 n);
 mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, i64 m, i64 k,
                          i64 n, void *ws, size_t ws_bytes, cudaStream_t s);

@@ -9,6 +9,8 @@ u64 stream_key(u64 seed, u64 stream);
 
 mela_status launch_rand_dense(u64 seed, u64 stream_id, i64 m, i64 n, u64 *out, i64 ld,
                               cudaStream_t s);
+mela_status launch_rand_bernoulli(u64 seed, u64 stream_id, i64 m, i64 n, double density, u64 *out,
+                                  i64 ld, cudaStream_t s);
 mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, cudaStream_t s);
 mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *out, cudaStream_t s);
 mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *out, i64 ld_out,
@@ -28,5 +30,10 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
                            i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s);
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                              i64 m, i64 k, i64 n, cudaStream_t s);
+
+// Whole RREF of one matrix in one single-CTA launch (batch.cu).
+size_t fused_workspace(i64 m, i64 n);
+mela_status launch_fused_elim(u64 *M, i64 ld, i64 m, i64 n, long long *d_rank, long long *d_piv,
+                              long long *d_prow, void *ws, size_t ws_bytes, cudaStream_t s);
 
 }  // namespace mela

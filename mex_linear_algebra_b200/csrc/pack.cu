@@ -48,6 +48,28 @@ __global__ void rand_dense_kernel(u64 key, i64 m, i64 n, i64 wc, u64 *out, i64 l
     }
 }
 
+// Bernoulli(density) bits: entry e = i*n + j takes 16-bit slice e%4 of word
+// e/4 of the stream and is 1 when the slice is below `thresh` (density*65536).
+__global__ void rand_bernoulli_kernel(u64 key, i64 m, i64 n, unsigned thresh, u64 *out, i64 ld)
+{
+    const i64 wc = words_of(n);
+    const i64 total = m * ld;
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
+        const i64 i = t / ld, w = t - i * ld;
+        u64 v = 0;
+        if (w < wc) {
+            const int cols = (n - 64 * w) < 64 ? (int)(n - 64 * w) : 64;
+            for (int b = 0; b < cols; ++b) {
+                const i64 e = i * n + 64 * w + b;
+                const u64 word = mix64(key + (u64)(e / 4 + 1) * 0x9E3779B97F4A7C15ULL);
+                const unsigned sl = (unsigned)(word >> (16 * (e & 3))) & 0xFFFFu;
+                if (sl < thresh) v |= 1ull << b;
+            }
+        }
+        out[t] = v;
+    }
+}
+
 // ---------------------------------------------------------------- pack
 // Parity of a double as the reference reads it, ((int)x) & 1, with the
 // x86-64 result for NaN and out-of-range values (INT_MIN, even) spelled out.
@@ -220,6 +242,18 @@ mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *ou
     return MELA_OK;
 }
 
+mela_status launch_rand_bernoulli(u64 seed, u64 stream_id, i64 m, i64 n, double density, u64 *out,
+                                  i64 ld, cudaStream_t s)
+{
+    if (m <= 0 || ld <= 0) return MELA_OK;
+    double t = density * 65536.0;
+    unsigned thresh = t <= 0 ? 0u : (t >= 65536.0 ? 65536u : (unsigned)t);
+    rand_bernoulli_kernel<<<grid_for(m * ld, 256), 256, 0, s>>>(stream_key(seed, stream_id), m, n, thresh,
+                                                                 out, ld);
+    MELA_LAUNCH_CHECK("rand_bernoulli_kernel");
+    return MELA_OK;
+}
+
 mela_status launch_rand_dense(u64 seed, u64 stream_id, i64 m, i64 n, u64 *out, i64 ld,
                               cudaStream_t s)
 {
@@ -243,6 +277,17 @@ extern "C" mela_status mela_dev_rand_dense(uint64_t seed, uint64_t stream_id, in
         return MELA_ERR_INVALID;
     }
     return launch_rand_dense(seed, stream_id, m, n, (u64 *)d_out, ld, (cudaStream_t)stream);
+}
+
+extern "C" mela_status mela_dev_rand_bernoulli(uint64_t seed, uint64_t stream_id, int64_t m,
+                                               int64_t n, double density, uint64_t *d_out, int64_t ld,
+                                               void *stream)
+{
+    if (m < 0 || n < 0 || ld < words_of(n) || (m > 0 && ld > 0 && !d_out) || !(density >= 0.0)) {
+        set_error("mela_dev_rand_bernoulli: bad shape, pointer or density");
+        return MELA_ERR_INVALID;
+    }
+    return launch_rand_bernoulli(seed, stream_id, m, n, density, (u64 *)d_out, ld, (cudaStream_t)stream);
 }
 
 extern "C" mela_status mela_dev_pack(int32_t kind, int64_t m, int64_t n, const void *d_in,

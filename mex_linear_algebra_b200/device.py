@@ -145,6 +145,13 @@ class BatchPlan:
                                                  1 if use_graph else 0, _stream(stream)))
         return ranks, zt
 
+    def unpack_logical(self, d_packed, out=None, stream=None):
+        """All matrices from packed rows to their logical column-major bytes."""
+        out = torch.empty(max(self.logical_bytes, 1), dtype=torch.uint8, device=d_packed.device) \
+            if out is None else out
+        check(lib().mela_batch_unpack_logical(self._plan, _ptr(d_packed), _ptr(out), _stream(stream)))
+        return out
+
     def basis(self, zt_host, ranks_host, i):
         """Packed basis of matrix i (nullity x ceil(n/64) uint64) from host copies."""
         n = int(self.shapes[i, 1])

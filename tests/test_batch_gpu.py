@@ -78,6 +78,8 @@ def test_logical_input(cuda):
     plan = D.BatchPlan([(m, n) for (m, n, _) in mats])
     chunks = [np.asfortranarray(O.unpack(P, m, n)).ravel(order="F").view(np.uint8) for (m, n, P) in mats]
     d_log = torch.from_numpy(np.concatenate(chunks)).cuda()
+    # the batched unpack produces the same logical bytes from the packed form
+    assert torch.equal(plan.unpack_logical(_pack_buffer(plan, mats)), d_log)
     ranks, zt = plan.run_logical(d_log)
     _check(plan, ranks, zt, mats)
     plan.close()

@@ -15,7 +15,7 @@ from gpu_util import to_dev, to_host, valid_words
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ("plain", "m4ri")
+FORMS = ("plain", "m4ri", "m4ri_k4", "fused")
 
 
 def dev_rref(P, m, n, form, rref=True):

@@ -142,3 +142,14 @@ def test_large_config_checks(cuda):
     del c_plain
     torch.cuda.empty_cache()
     assert D.device_error_flags() == 0
+
+
+def test_bernoulli_generator_matches_host(cuda):
+    import torch
+    from mex_linear_algebra_b200 import _lib, gen
+    L = _lib.lib()
+    for (m, n, d, st) in [(7, 70, 0.1, 1), (100, 300, 0.003, 2), (33, 64, 0.5, 3)]:
+        out = torch.empty((m, (n + 63) // 64), dtype=torch.int64, device="cuda")
+        _lib.check(L.mela_dev_rand_bernoulli(4, st, m, n, d, out.data_ptr(), out.shape[1],
+                                             torch.cuda.current_stream().cuda_stream))
+        assert np.array_equal(to_host(out), gen.sparse_packed(4, st, m, n, d))
