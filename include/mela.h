@@ -69,7 +69,9 @@ typedef enum {
     MELA_GEMM_AUTO = 0,
     MELA_GEMM_PLAIN = 1,  /* bit-packed AND + popcount parity on CUDA cores */
     MELA_GEMM_M4RI = 2,   /* Four-Russians tables in shared memory */
-    MELA_GEMM_TC = 3      /* tcgen05 kind::i8 tensor cores, parity of the s32 sum */
+    MELA_GEMM_TC = 3,     /* tcgen05 kind::i8 tensor cores, parity of the s32 sum */
+    MELA_GEMM_TC_FP4 = 4  /* tcgen05 kind::mxf4 (e2m1 0/1, unit scales), parity of the exact
+                             f32 sum; k < 2^24 */
 } mela_gemm_variant;
 
 /* Elimination variants (rank / RREF / null space); results are identical. */
@@ -281,7 +283,7 @@ mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_p
  * shape and density; the dispatcher takes the fastest prediction.  It only
  * chooses how a result is computed: every variant returns the same bits.
  * Parameters: one float array W1[8][32] b1[32] W2[32][32] b2[32] W3[32][4]
- * b3[4].  Variant order per output: products (plain, m4ri, tc, -); rank and
+ * b3[4].  Variant order per output: products (plain, m4ri, tc, tc_fp4); rank and
  * null space (plain, m4ri, m4ri_k4, fused). */
 #define MELA_MLP_IN 8
 #define MELA_MLP_H1 32

@@ -17,8 +17,9 @@ OK, ERR_INVALID, ERR_SPARSE, ERR_DIM, ERR_TYPE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT
 # mela_kind
 KIND_LOGICAL, KIND_DOUBLE, KIND_OTHER = 0, 1, 2
 # mela_gemm_variant
-GEMM_AUTO, GEMM_PLAIN, GEMM_M4RI, GEMM_TC = 0, 1, 2, 3
-GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc": GEMM_TC}
+GEMM_AUTO, GEMM_PLAIN, GEMM_M4RI, GEMM_TC, GEMM_TC_FP4 = 0, 1, 2, 3, 4
+GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc": GEMM_TC,
+                 "tc_fp4": GEMM_TC_FP4}
 
 
 # mela_function (gateway ids)
@@ -27,7 +28,7 @@ FN_MATMUL_GF2, FN_MATMUL_M4RI, FN_RANK_GF2, FN_RANK_M4RI, FN_NULL_GF2, FN_NULL_M
 OP_RANK, OP_NULL, OP_MATMUL = 0, 1, 2
 MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 4, 1476
 # variant index (model output) -> variant code, per op
-OP_VARIANTS = {OP_MATMUL: (1, 2, 3), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
+OP_VARIANTS = {OP_MATMUL: (1, 2, 3, 4), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
 # mela_elim_variant
 ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI, ELIM_M4RI_K4, ELIM_FUSED = 0, 1, 2, 3, 4
 ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI, "m4ri_k4": ELIM_M4RI_K4,

@@ -44,7 +44,8 @@ def time_matmul(torch, m, k, n, density, stream_id, reps=3):
     B = _bernoulli(torch, SEED, 2 * stream_id + 1, k, n, density)
     wn = (n + 63) // 64
     times, outs = {}, {}
-    for v, name in zip((_lib.GEMM_PLAIN, _lib.GEMM_M4RI, _lib.GEMM_TC), VARIANT_NAMES["matmul"]):
+    for v, name in zip((_lib.GEMM_PLAIN, _lib.GEMM_M4RI, _lib.GEMM_TC, _lib.GEMM_TC_FP4),
+                       VARIANT_NAMES["matmul"]):
         wsb = L.mela_matmul_workspace_size(v, m, k, n)
         ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
         C_ = torch.empty((m, wn), dtype=torch.int64, device="cuda")

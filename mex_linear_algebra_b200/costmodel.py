@@ -23,7 +23,7 @@ from ._lib import check, lib
 PKG = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(PKG, "costmodel.json")
 OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL}
-VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc"), "rank": ("plain", "m4ri", "m4ri_k4", "fused"),
+VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc", "tc_fp4"), "rank": ("plain", "m4ri", "m4ri_k4", "fused"),
                  "null": ("plain", "m4ri", "m4ri_k4", "fused")}
 
 

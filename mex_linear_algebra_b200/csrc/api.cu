@@ -154,7 +154,12 @@ int choose_gemm_variant(i64 m, i64 k, i64 n)
 {
     // the learned cost model when one is installed (dense input assumed)
     const int c = costmodel_choose(MELA_OP_MATMUL, (double)m, (double)k, (double)n, 0.5);
-    if (c >= 0) return c == 0 ? MELA_GEMM_PLAIN : (c == 1 ? MELA_GEMM_M4RI : MELA_GEMM_TC);
+    if (c >= 0) {
+        static const int order[4] = {MELA_GEMM_PLAIN, MELA_GEMM_M4RI, MELA_GEMM_TC, MELA_GEMM_TC_FP4};
+        const int v = order[c & 3];
+        if (v == MELA_GEMM_TC_FP4 && k >= (1LL << 24)) return MELA_GEMM_TC;
+        return v;
+    }
     // fixed rule: tensor cores pay off once every dimension spans a few
     // tiles; below that the expansion to bytes dominates
     if (m >= 1024 && n >= 1024 && k >= 1024) return MELA_GEMM_TC;
@@ -167,11 +172,19 @@ static GemmPlan plan_gemm(int variant, i64 m, i64 k, i64 n)
     if (variant == MELA_GEMM_AUTO) variant = choose_gemm_variant(m, k, n);
     p.variant = variant;
     p.ldbt = even_words(k);
-    if (variant == MELA_GEMM_PLAIN || variant == MELA_GEMM_TC) p.bt_bytes = (size_t)n * p.ldbt * 8;
+    if (variant == MELA_GEMM_PLAIN || variant == MELA_GEMM_TC || variant == MELA_GEMM_TC_FP4)
+        p.bt_bytes = (size_t)n * p.ldbt * 8;
     if (variant == MELA_GEMM_TC) {
         p.mp = round_up(m, 128);
         p.np = round_up(n, 256);
-        p.kp = round_up(k, 128);
+        p.kp = round_up(k, 128);  // bytes = values
+        p.a8_bytes = (size_t)p.mp * p.kp;
+        p.b8_bytes = (size_t)p.np * p.kp;
+    }
+    if (variant == MELA_GEMM_TC_FP4) {
+        p.mp = round_up(m, 128);
+        p.np = round_up(n, 256);
+        p.kp = round_up(k, 256) / 2;  // bytes, two values each
         p.a8_bytes = (size_t)p.mp * p.kp;
         p.b8_bytes = (size_t)p.np * p.kp;
     }
@@ -215,7 +228,11 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
     mela_status st = check_ws(p, ws, ws_bytes);
     if (st != MELA_OK) return st;
     GemmBufs b = carve(p, ws);
-    if (p.variant == MELA_GEMM_PLAIN || p.variant == MELA_GEMM_TC) {
+    if (p.variant == MELA_GEMM_TC_FP4 && k >= (1LL << 24)) {
+        set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+        return MELA_ERR_UNSUPPORTED;
+    }
+    if (p.variant == MELA_GEMM_PLAIN || p.variant == MELA_GEMM_TC || p.variant == MELA_GEMM_TC_FP4) {
         if ((st = launch_transpose(B, ldb, k, n, b.Bt, p.ldbt, s)) != MELA_OK) return st;
         if (p.ldbt > words_of(k)) {
             // the pad word of each Bt row must read as zero
@@ -225,6 +242,10 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
     if (p.variant == MELA_GEMM_TC) {
         if ((st = launch_expand_u8(A, lda, m, k, p.mp, p.kp, b.A8, s)) != MELA_OK) return st;
         if ((st = launch_expand_u8(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)) != MELA_OK) return st;
+    }
+    if (p.variant == MELA_GEMM_TC_FP4) {
+        if ((st = launch_expand_f4(A, lda, m, k, p.mp, p.kp, b.A8, s)) != MELA_OK) return st;
+        if ((st = launch_expand_f4(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)) != MELA_OK) return st;
     }
     return MELA_OK;
 }
@@ -244,7 +265,13 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
     GemmBufs b = carve(p, ws);
     switch (p.variant) {
     case MELA_GEMM_PLAIN: return launch_gemm_plain(A, lda, b.Bt, p.ldbt, C, ldc, m, k, n, s);
-    case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s);
+    case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, false);
+    case MELA_GEMM_TC_FP4:
+        if (k >= (1LL << 24)) {
+            set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+            return MELA_ERR_UNSUPPORTED;
+        }
+        return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, true);
     case MELA_GEMM_M4RI: return launch_gemm_m4ri(A, lda, B, ldb, C, ldc, m, k, n, s);
     default:
         set_error("unknown product variant %d", p.variant);
@@ -325,7 +352,7 @@ extern "C" mela_status mela_device_error_flags(uint32_t *flags, int clear)
 
 extern "C" size_t mela_matmul_workspace_size(int32_t variant, int64_t m, int64_t k, int64_t n)
 {
-    if (variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC) return 0;
+    if (variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4) return 0;
     return gemm_workspace(variant, m, k, n);
 }
 
@@ -334,7 +361,7 @@ extern "C" mela_status mela_dev_matmul(int32_t variant, const uint64_t *dA, int6
                                        int64_t m, int64_t k, int64_t n, void *workspace,
                                        size_t workspace_bytes, void *stream)
 {
-    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC ||
+    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4 ||
         lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
         set_error("mela_dev_matmul: bad shape, leading dimension or variant");
         return MELA_ERR_INVALID;
@@ -351,7 +378,7 @@ static mela_status check_dev_matmul_args(int32_t variant, const uint64_t *dA, in
                                          const uint64_t *dB, int64_t ldb, int64_t ldc, int64_t m,
                                          int64_t k, int64_t n)
 {
-    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC ||
+    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4 ||
         lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
         set_error("bad shape, leading dimension or variant");
         return MELA_ERR_INVALID;
@@ -394,7 +421,7 @@ extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, c
                                                int64_t k, int64_t n, int32_t variant)
 {
     if (m < 0 || k < 0 || n < 0 || lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n) ||
-        variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC) {
+        variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4) {
         set_error("mela_matmul_packed_host: bad shape or variant");
         return MELA_ERR_INVALID;
     }

@@ -17,6 +17,14 @@
 //                    packed words per row.
 // Tiles are rasterised in bands of 16 tile-rows so that the CTAs resident
 // at one time share A and B tiles in L2.
+//
+// FP4 form (F4 = true): the operands are packed E2M1 values (0x2 = 1.0,
+// 0x0 = 0; two per byte), the instruction is tcgen05 kind::mxf4 with one
+// UE8M0 scale factor per 32 values of K, at twice the INT8 rate.  Every scale
+// factor is 1.0, so the scale-factor columns of TMEM are one constant block
+// (bytes 0x7F) written once per CTA and addressed by every instruction.  The
+// f32 accumulator holds the integer dot product exactly while it is below
+// 2^24, so K < 2^24 is required; the parity bit is that of the integer.
 #include "mela_common.cuh"
 #include "mela_internal.h"
 #include "tc_ptx.cuh"
@@ -31,7 +39,7 @@ constexpr int A_BYTES = BM * BK;
 constexpr int B_BYTES = BN * BK;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr u32 TMEM_COLS = 256;
+constexpr u32 SF_COL = 256;   // first TMEM column of the 32 constant scale-factor columns (FP4 form)
 constexpr int GROUP_M = 16;
 
 struct Ctl {
@@ -45,11 +53,13 @@ struct Ctl {
 
 }  // namespace
 
+template <bool F4>
 __global__ void __launch_bounds__(192, 1)
 gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                u64 *__restrict__ C, i64 ldc, i64 m, i64 n, int tiles_m, int tiles_n, int kstages,
                u32 *err)
 {
+    constexpr u32 TMEM_COLS = F4 ? 512 : 256;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem =
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -89,6 +99,18 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     ptx::tc_fence_after();
     const u32 tmem = ctl->tmem;
     volatile int *abort_flag = &ctl->abort;
+    if constexpr (F4) {
+        // constant scale factors: every byte of columns SF_COL.. = 0x7F (2^0)
+        if (warp >= 2) {
+            const u32 lane_base = (u32)((warp & 3) * 32) << 16;
+            ptx::tmem_st_32x32b_x16(tmem + lane_base + SF_COL, 0x7F7F7F7Fu);
+            ptx::tmem_st_32x32b_x16(tmem + lane_base + SF_COL + 16, 0x7F7F7F7Fu);
+            ptx::tmem_st_wait();
+        }
+        ptx::tc_fence_before();
+        __syncthreads();
+        ptx::tc_fence_after();
+    }
 
     if (warp == 0) {
         if (lane == 0) {
@@ -116,7 +138,7 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr u32 idesc = ptx::idesc_i8(BM, BN);
+            constexpr u32 idesc = F4 ? ptx::idesc_mxf4(BM, BN) : ptx::idesc_i8(BM, BN);
             bool ok = true;
             for (int ks = 0; ks < kstages; ++ks) {
                 const int s = ks % STAGES, round = ks / STAGES;
@@ -129,9 +151,15 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 const u32 a0 = ptx::smem_u32(smem + s * STAGE_BYTES);
                 const u32 b0 = a0 + A_BYTES;
 #pragma unroll
-                for (int kk = 0; kk < BK / 32; ++kk)
-                    ptx::umma_i8(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
-                                 idesc, (ks | kk) != 0);
+                for (int kk = 0; kk < BK / 32; ++kk) {
+                    // 32 bytes of K per instruction: 32 int8 values or 64 packed e2m1 values
+                    if constexpr (F4)
+                        ptx::umma_mxf4(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
+                                       idesc, tmem + SF_COL, tmem + SF_COL + 8, (ks | kk) != 0);
+                    else
+                        ptx::umma_i8(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
+                                     idesc, (ks | kk) != 0);
+                }
                 ptx::umma_commit(&ctl->empty[s]);
             }
             if (ok) {
@@ -158,7 +186,10 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 ptx::tmem_ld_wait();
                 u32 b = 0;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) b |= (r[j] & 1u) << j;
+                for (int j = 0; j < 32; ++j) {
+                    const u32 v = F4 ? (u32)__float2int_rz(__uint_as_float(r[j])) : r[j];
+                    b |= (v & 1u) << j;
+                }
                 bits[c] = b;
             }
             const i64 nw = words_of(n);
@@ -224,7 +255,7 @@ static mela_status make_map(CUtensorMap *map, const unsigned char *base, i64 row
 }
 
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
-                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s)
+                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4)
 {
     if (m <= 0 || n <= 0) return MELA_OK;
     if (mp % BM || np % BN || kp % BK || kp <= 0) {
@@ -245,14 +276,17 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
     if (st != MELA_OK) return st;
     st = make_map(&mb, Bt8, np, kp, BN);
     if (st != MELA_OK) return st;
-    static bool attr_set = false;
-    if (!attr_set) {
-        MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (fp4) {
+        MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            SMEM_BYTES));
-        attr_set = true;
+        gemm_tc_kernel<true><<<(unsigned)(tiles_m * tiles_n), 192, SMEM_BYTES, s>>>(
+            ma, mb, C, ldc, m, n, (int)tiles_m, (int)tiles_n, (int)kst, device_error_word());
+    } else {
+        MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           SMEM_BYTES));
+        gemm_tc_kernel<false><<<(unsigned)(tiles_m * tiles_n), 192, SMEM_BYTES, s>>>(
+            ma, mb, C, ldc, m, n, (int)tiles_m, (int)tiles_n, (int)kst, device_error_word());
     }
-    gemm_tc_kernel<<<(unsigned)(tiles_m * tiles_n), 192, SMEM_BYTES, s>>>(
-        ma, mb, C, ldc, m, n, (int)tiles_m, (int)tiles_n, (int)kst, device_error_word());
     MELA_LAUNCH_CHECK("gemm_tc_kernel");
     return MELA_OK;
 }

@@ -15,6 +15,8 @@ mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld
 mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *out, cudaStream_t s);
 mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *out, i64 ld_out,
                              cudaStream_t s);
+mela_status launch_expand_f4(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad_bytes,
+                             unsigned char *out, cudaStream_t s);
 mela_status launch_expand_u8(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad,
                              unsigned char *out, cudaStream_t s);
 
@@ -26,8 +28,9 @@ mela_status launch_gemm_plain(const u64 *A, i64 lda, const u64 *Bt, i64 ldbt, u6
 // Tensor-core product on 0/1 byte operands A8 (mp x kp) and Bt8 (np x kp),
 // both K-major; mp % 128 == 0, np % 256 == 0, kp % 128 == 0.  Writes the
 // valid m x n block of packed C.
+// fp4 = true: packed e2m1 operands (kp counts bytes, two values each), kind::mxf4.
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
-                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s);
+                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4);
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                              i64 m, i64 k, i64 n, cudaStream_t s);
 

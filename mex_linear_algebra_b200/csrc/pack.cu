@@ -190,6 +190,37 @@ __global__ void __launch_bounds__(256) expand_u8_kernel(const u64 *__restrict__ 
     }
 }
 
+// out (rows_pad x kpad_bytes, two e2m1 values per byte): value k of row r is
+// 1.0 (0x2) when bit k of packed row r is set, else 0; element 2j in the low
+// nibble of byte j.  One thread per 64-bit word -> 32 bytes.
+__device__ __forceinline__ u32 spread_even4(u32 v)  // bits 0,2,4,6 -> bit 0 of bytes 0..3
+{
+    return (v & 1u) | ((v & 4u) << 6) | ((v & 16u) << 12) | ((v & 64u) << 18);
+}
+
+__global__ void __launch_bounds__(256) expand_f4_kernel(const u64 *__restrict__ in, i64 ld, i64 rows,
+                                                        i64 kbits, i64 rows_pad, i64 kpad_bytes,
+                                                        unsigned char *__restrict__ out)
+{
+    const i64 wpr = kpad_bytes >> 5;  // 64-bit source words per padded row
+    const i64 total = rows_pad * wpr;
+    const i64 wc = words_of(kbits);
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < total;
+         t += (i64)gridDim.x * blockDim.x) {
+        const i64 r = t / wpr, w = t - r * wpr;
+        const u64 v = (r < rows && w < wc) ? in[r * ld + w] : 0ull;
+        u32 o[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const u32 x = (u32)(v >> (8 * q)) & 0xFFu;
+            o[q] = (spread_even4(x & 0x55u) << 1) | (spread_even4((x >> 1) & 0x55u) << 5);
+        }
+        uint4 *dst = reinterpret_cast<uint4 *>(out + r * kpad_bytes + w * 32);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static int grid_for(i64 total, int threads)
 {
@@ -206,6 +237,15 @@ mela_status launch_expand_u8(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 row
     i64 total = rows_pad * (kpad >> 6);
     expand_u8_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, ld, rows, kbits, rows_pad, kpad, out);
     MELA_LAUNCH_CHECK("expand_u8_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_expand_f4(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad_bytes,
+                             unsigned char *out, cudaStream_t s)
+{
+    i64 total = rows_pad * (kpad_bytes >> 5);
+    expand_f4_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, ld, rows, kbits, rows_pad, kpad_bytes, out);
+    MELA_LAUNCH_CHECK("expand_f4_kernel");
     return MELA_OK;
 }
 

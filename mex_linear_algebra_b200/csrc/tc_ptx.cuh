@@ -117,6 +117,29 @@ __device__ __forceinline__ void umma_i8(u32 d_tmem, u64 a_desc, u64 b_desc, u32 
         : "memory");
 }
 
+// D[tmem] (+)= (A * sfa) x (B * sfb)^T, kind::mxf4 (packed e2m1 operands,
+// one UE8M0 scale per 32 values of K), one CTA.
+__device__ __forceinline__ void umma_mxf4(u32 d_tmem, u64 a_desc, u64 b_desc, u32 idesc, u32 sfa_tmem,
+                                          u32 sfb_tmem, u32 accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(sfa_tmem), "r"(sfb_tmem)
+        : "memory");
+}
+
+// 32 lanes x 16 consecutive 32-bit columns from registers.
+__device__ __forceinline__ void tmem_st_32x32b_x16(u32 taddr, u32 v)
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr), "r"(v)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // Arrive on `bar` once every previously issued UMMA of this thread completes.
 __device__ __forceinline__ void umma_commit(u64 *bar)
 {
@@ -159,6 +182,20 @@ __host__ __device__ constexpr u32 idesc_i8(int M, int N)
     return (2u << 4)                 // D format: s32
            | (0u << 7) | (0u << 10)  // A, B: unsigned 8-bit
            | ((u32)(N >> 3) << 17) | ((u32)(M >> 4) << 24);
+}
+
+// Instruction descriptor, kind::mxf4 block-scaled: E2M1 A and B (K-major),
+// UE8M0 scale factors (scale-factor byte 0 of the addressed cells), f32
+// accumulator, K = 64 per instruction, M x N.
+__host__ __device__ constexpr u32 idesc_mxf4(int M, int N)
+{
+    return (0u << 4)                 // B scale-factor byte id
+           | (1u << 7) | (1u << 10)  // A, B: E2M1
+           | ((u32)(N >> 3) << 17)   //
+           | (1u << 23)              // scale format: UE8M0
+           | ((u32)(M >> 4) << 24)   //
+           | (0u << 29)              // A scale-factor byte id
+           | (0u << 31);             // K = 64 (dense)
 }
 
 }  // namespace ptx

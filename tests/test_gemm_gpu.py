@@ -14,7 +14,7 @@ from gpu_util import to_dev, to_host, valid_words
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = ("plain", "m4ri", "tc")
+VARIANTS = ("plain", "m4ri", "tc", "tc_fp4")
 
 
 def _dev():
@@ -153,3 +153,33 @@ def test_bernoulli_generator_matches_host(cuda):
         _lib.check(L.mela_dev_rand_bernoulli(4, st, m, n, d, out.data_ptr(), out.shape[1],
                                              torch.cuda.current_stream().cuda_stream))
         assert np.array_equal(to_host(out), gen.sparse_packed(4, st, m, n, d))
+
+
+@pytest.mark.parametrize("k", [1, 63, 255, 257, 32767, 32769, 1048577])
+def test_long_sums_exact(cuda, k):
+    """All-ones operands: every entry of C is k mod 2, the sum of k ones.
+    Checks that the tensor-core forms keep the integer sum exact (the fp4 form
+    accumulates in f32, exact below 2^24)."""
+    import torch
+    D = _dev()
+    m, n = 256, 256
+    wk, wn = (k + 63) // 64, (n + 63) // 64
+    A = torch.zeros((m, wk), dtype=torch.int64, device="cuda")
+    B = torch.zeros((k, wn), dtype=torch.int64, device="cuda")
+    A[:] = -1
+    B[:] = -1
+    if k % 64:
+        A[:, -1] = (1 << (k % 64)) - 1
+    want = np.uint64(0xFFFFFFFFFFFFFFFF) if (k & 1) else np.uint64(0)
+    for variant in ("tc", "tc_fp4", "plain"):
+        C = to_host(D.matmul(A, B, m, k, n, variant=variant))
+        assert (C == want).all(), (variant, k)
+
+
+def test_fp4_variants_agree_large(cuda):
+    import torch
+    D = _dev()
+    m, k, n = 8192, 16384, 8192
+    A = D.rand_dense(13, 0, m, k)
+    B = D.rand_dense(13, 1, k, n)
+    assert torch.equal(D.matmul(A, B, m, k, n, variant="tc_fp4"), D.matmul(A, B, m, k, n, variant="tc"))
