@@ -80,7 +80,8 @@ typedef enum {
     MELA_ELIM_PLAIN = 1,  /* per-pivot warp-ballot search + broadcast-XOR sweep */
     MELA_ELIM_M4RI = 2,   /* 64-column panels, 8-bit Gray-code tables in shared memory */
     MELA_ELIM_M4RI_K4 = 3, /* the same panels with 4-bit tables (M4RI k = 4) */
-    MELA_ELIM_FUSED = 4    /* the whole elimination by one CTA in one launch */
+    MELA_ELIM_FUSED = 4,   /* the whole elimination by one CTA in one launch */
+    MELA_ELIM_TC = 5       /* 256-column windows, trailing update on the tensor cores (tcgen05 kind::i8) */
 } mela_elim_variant;
 
 /* ------------------------------------------------------------------ */

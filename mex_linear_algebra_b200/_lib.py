@@ -30,9 +30,9 @@ MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 4, 1476
 # variant index (model output) -> variant code, per op
 OP_VARIANTS = {OP_MATMUL: (1, 2, 3, 4), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
 # mela_elim_variant
-ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI, ELIM_M4RI_K4, ELIM_FUSED = 0, 1, 2, 3, 4
+ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI, ELIM_M4RI_K4, ELIM_FUSED, ELIM_TC = 0, 1, 2, 3, 4, 5
 ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI, "m4ri_k4": ELIM_M4RI_K4,
-                 "fused": ELIM_FUSED}
+                 "fused": ELIM_FUSED, "tc": ELIM_TC}
 
 
 class GatewayError(C.Structure):

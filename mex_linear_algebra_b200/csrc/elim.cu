@@ -539,8 +539,9 @@ ElimLayout elim_layout(i64 m, i64 n)
 
 size_t elim_workspace(i64 m, i64 n)
 {
-    const size_t a = elim_layout(m, n).total, b = fused_workspace(m, n);
-    return a > b ? a : b;
+    const size_t a = elim_layout(m, n).total, b = fused_workspace(m, n), c = elim_tc_workspace(m, n);
+    const size_t ab = a > b ? a : b;
+    return ab > c ? ab : c;
 }
 
 int choose_elim_variant(i64 m, i64 n, int rref)
@@ -566,6 +567,7 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
     }
     if (variant == MELA_ELIM_FUSED)
         return launch_fused_elim(M, ld, m, n, d_rank, d_piv, d_prow, ws, ws_bytes, s);
+    if (variant == MELA_ELIM_TC) return elim_tc_device(M, ld, m, n, rref, d_rank, d_piv, d_prow, ws, ws_bytes, s);
     ElimLayout L = elim_layout(m, n);
     if (ws_bytes < L.total || !ws) {
         set_error("elimination workspace of %zu bytes needed, %zu given", elim_workspace(m, n), ws_bytes);

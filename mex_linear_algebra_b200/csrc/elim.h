@@ -24,6 +24,11 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
                         long long *d_piv, long long *d_prow, void *ws, size_t ws_bytes,
                         cudaStream_t s);
 
+// Tensor-core form (elim_tc.cu): same contract as elim_device.
+size_t elim_tc_workspace(i64 m, i64 n);
+mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank, long long *d_piv,
+                           long long *d_prow, void *ws, size_t ws_bytes, cudaStream_t s);
+
 NullLayout null_layout(i64 n, i64 rank);
 // Null-space basis from an RREF: Zt row i = e_{f_i} + sum_p R_p[f_i] e_{piv[p]},
 // free columns f_i ascending (n - rank rows of ldz words).

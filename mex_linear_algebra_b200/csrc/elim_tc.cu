@@ -1,0 +1,940 @@
+// elim_tc.cu -- blocked GF(2) elimination whose trailing (Schur) update runs
+// on the sm_100a tensor cores.
+//
+// Results are those of the other forms (elim.cu): the rank of
+// bitrank_packed / rank_m4ri (src/mela_rank_gf2.c:27-121,
+// src/mela_rank_m4ri.c:94-279), the greedy pivot columns and the unique RREF
+// rows of gf2_rref_standard (src/mela_null_gf2.c:88-131).  Rows never move:
+// pivot t lives in physical row prow[t].
+//
+// One window of 256 columns (4 words) at a time:
+//   window_factor   one CTA.  Walks the list of active rows in chunks of 320.
+//                   Each row's window part is reduced by the basis found so
+//                   far (reduced row echelon, lowest set bit leading) through
+//                   64 tables of the 16 combinations of 4 basis vectors; the
+//                   rows left nonzero are eliminated among themselves by a
+//                   CTA-wide Gauss-Jordan (a thread per row, one barrier per
+//                   pivot: the next pivot is the row with the lowest leading
+//                   bit, found by a warp min-reduction and a shared-memory
+//                   atomicMin); the older basis vectors are then reduced by the
+//                   new ones.  Every basis vector carries its combination
+//                   ("tag") over the rows P_j that entered the basis, so
+//                   R_window = T * A[P, window].  The walk stops as soon as the
+//                   basis spans every column of the window.  The walked part of
+//                   the list is then compacted in place (pivot rows and rows
+//                   found zero from the window on are dropped, order kept).
+//   window_combine  R_t = sum_j T[t][j] A[P_j] over the words from the window
+//                   on, into the panel buffer (a warp per t, a lane per word).
+//   window_coef     every other row to update (rank: the active rows; RREF: all
+//                   rows) whose bits at the window's pivot columns are not all
+//                   zero gets a slot; those bits become a row of 0/1 bytes.
+//   window_rt       R transposed as 0/1 bytes, Rt8[j][t] = bit j of R_t, and
+//                   R_t written over row P_t.
+//   tc_update       A[row(slot), w..] ^= parity(X8[slot] . Rt8^T): tcgen05
+//                   kind::i8 128 x 256 tiles with K = 256.  A persistent CTA
+//                   keeps 256-column strips of Rt8 in shared memory (two
+//                   buffers) and streams 128-row tiles of X8 through a 2-stage
+//                   ring into two TMEM accumulators; four epilogue warps XOR the
+//                   parity bits into the packed rows while the next tile is
+//                   multiplied, and flag the rows that are still nonzero.
+// Since the basis is reduced, a row's coefficient for R_t is its own bit at
+// pivot column t, and XORing sum_t x_t R_t clears every pivot column of the
+// window; a row whose window part lies in the basis' span (every active row,
+// once the scan has ended) is then zero across the window.
+#include <climits>
+
+#include "mela_common.cuh"
+#include "mela_internal.h"
+#include "mela_host.h"
+#include "elim.h"
+#include "tc_ptx.cuh"
+
+namespace mela {
+
+namespace {
+
+constexpr int WW = 4;         // words per window
+constexpr int WBITS = 256;    // columns per window
+constexpr int WF_THREADS = 320;  // a chunk of rows; 320 random rows span 256 columns but with probability 2^-64
+
+struct WinState {
+    long long rank;         // pivots so far (every window)
+    int rt;                 // pivots of the current window
+    int nu;                 // rows to update in the current window
+    int na;                 // rows in the active-row list
+    int lbase;              // the list is list[lbase .. lbase + na)
+    u64 have[WW];           // window-relative pivot columns
+    int prow[WBITS];        // physical row of P-index j
+    u64 tag[WBITS][WW];     // pivot t (ascending column): R_t = sum_j bit j * A[prow[j]]
+};
+
+struct WfSmem {
+    u64 bd[WBITS][WW];        // basis vector whose leading bit is b
+    u64 bt[WBITS][WW];        // its tag
+    u64 tab[64][16][WW];      // nibble tables of the basis
+    u64 tabt[64][16][WW];     // the same over the tags
+    u64 cx[WF_THREADS][WW];   // rows of the current chunk (residual)
+    u64 ct[WF_THREADS][WW];   //   and their tags
+    int newslot[WBITS];       // chunk slot of the k-th new basis vector
+    int newlead[WBITS];       //   and its leading bit
+    int prow[WBITS];          // physical row of P-index j
+    u64 have[WW];
+    unsigned keys[3];         // smallest key, rotating by iteration
+    int nb, cnt;
+    int wsum[32];
+};
+
+__device__ __forceinline__ int ctz64w(u64 x) { return __ffsll((long long)x) - 1; }
+
+// Word q of a 4-word vector held in registers (selects, no local memory).
+__device__ __forceinline__ u64 sel4(const u64 (&v)[WW], int q)
+{
+    return q == 0 ? v[0] : (q == 1 ? v[1] : (q == 2 ? v[2] : v[3]));
+}
+__device__ __forceinline__ bool bit_of(const u64 (&v)[WW], int b) { return (sel4(v, b >> 6) >> (b & 63)) & 1; }
+__device__ __forceinline__ void or_word(u64 (&v)[WW], int q, u64 x)
+{
+#pragma unroll
+    for (int i = 0; i < WW; ++i) v[i] |= (i == q) ? x : 0ull;
+}
+__device__ __forceinline__ void xor4s(u64 (&a)[WW], const u64 *b)
+{
+#pragma unroll
+    for (int q = 0; q < WW; ++q) a[q] ^= b[q];
+}
+__device__ __forceinline__ bool any4(const u64 (&v)[WW]) { return (v[0] | v[1] | v[2] | v[3]) != 0; }
+__device__ __forceinline__ int lead4(const u64 (&v)[WW])
+{
+    return v[0] ? ctz64w(v[0]) : (v[1] ? 64 + ctz64w(v[1]) : (v[2] ? 128 + ctz64w(v[2]) : 192 + ctz64w(v[3])));
+}
+
+// Exclusive position of this thread's flag among the block's flags (thread
+// order) and the block total; every thread of the block must call it.
+__device__ __forceinline__ int block_slot(bool flag, int *wsum, int &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) wsum[warp] = __popc(bal);
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, off);
+            if (lane >= off) v += u;
+        }
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    total = wsum[31];
+    const int slot = (warp ? wsum[warp - 1] : 0) + __popc(bal & ((1u << lane) - 1));
+    __syncthreads();  // wsum may be rewritten by the next call
+    return slot;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- window_factor
+__global__ void __launch_bounds__(WF_THREADS, 1)
+window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int *list, const unsigned char *live,
+                     unsigned char *state, int *stamp, int wid, WinState *ws, long long *piv, long long *prow)
+{
+    extern __shared__ __align__(16) unsigned char wf_raw[];
+    WfSmem &S = *reinterpret_cast<WfSmem *>(wf_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const i64 wc = words_of(n);
+    const int wn = (wc - w) < WW ? (int)(wc - w) : WW;
+    const i64 vb = n - 64 * w;
+    const int valid = vb < WBITS ? (int)vb : WBITS;  // columns of this window inside the matrix
+    const int na = ws->na;
+    int *L0 = list + ws->lbase;
+    constexpr unsigned NOKEY = 0xFFFFFFFFu;
+
+    for (int e = tid; e < 64 * 16 * WW; e += WF_THREADS) {
+        (&S.tab[0][0][0])[e] = 0;
+        (&S.tabt[0][0][0])[e] = 0;
+    }
+    if (tid < WW) S.have[tid] = 0;
+    if (tid == 0) S.nb = 0;
+    __syncthreads();
+
+    int walked = 0;
+    for (int base = 0; base < na; base += WF_THREADS) {
+        if (S.nb >= valid) break;
+        walked = base + WF_THREADS < na ? base + WF_THREADS : na;
+        const int nb0 = S.nb;
+        u64 hv[WW];
+#pragma unroll
+        for (int q = 0; q < WW; ++q) hv[q] = S.have[q];
+        const int k = base + tid;
+        int row = -1;
+        u64 x[WW] = {0, 0, 0, 0};
+        if (k < na) {
+            row = L0[k];
+#pragma unroll
+            for (int q = 0; q < WW; ++q)
+                if (q < wn) x[q] = M[(i64)row * ld + w + q];
+        }
+        u64 cx[WW] = {x[0], x[1], x[2], x[3]}, ct[WW] = {0, 0, 0, 0};
+        if (any4(x) && nb0) {
+#pragma unroll
+            for (int g = 0; g < 64; ++g) {
+                const int q = g >> 4, sh = 4 * (g & 15);
+                const u64 hn = (hv[q] >> sh) & 15;
+                if (hn) {
+                    const int nib = (int)((x[q] >> sh) & hn);
+                    if (nib) xor4s(cx, S.tab[g][nib]);
+                }
+            }
+            if (any4(cx)) {
+#pragma unroll
+                for (int g = 0; g < 64; ++g) {
+                    const int q = g >> 4, sh = 4 * (g & 15);
+                    const u64 hn = (hv[q] >> sh) & 15;
+                    if (hn) {
+                        const int nib = (int)((x[q] >> sh) & hn);
+                        if (nib) xor4s(ct, S.tabt[g][nib]);
+                    }
+                }
+            }
+        }
+        // Gauss-Jordan among the chunk's residual rows, a pivot per barrier.
+        // A row's key is (leading bit, slot); the next pivot is the smallest
+        // key.  Only the row holding its warp's smallest key publishes itself
+        // to shared memory, its tag already carrying the P-index it would
+        // enter as, so the pivot is always published.
+        bool used = false;
+        int myj = -1;
+        unsigned key = any4(cx) ? ((unsigned)lead4(cx) << 10 | (unsigned)tid) : NOKEY;
+        auto publish = [&](unsigned *kslot, int jn) {
+            const unsigned mk = __reduce_min_sync(0xffffffffu, key);
+            if (key == mk && key != NOKEY) {
+                ulonglong2 *dv = reinterpret_cast<ulonglong2 *>(S.cx[tid]);
+                ulonglong2 *dt = reinterpret_cast<ulonglong2 *>(S.ct[tid]);
+                const u64 e = 1ull << (jn & 63);
+                const int jq = jn >> 6;
+                dv[0] = make_ulonglong2(cx[0], cx[1]);
+                dv[1] = make_ulonglong2(cx[2], cx[3]);
+                dt[0] = make_ulonglong2(ct[0] ^ (jq == 0 ? e : 0ull), ct[1] ^ (jq == 1 ? e : 0ull));
+                dt[1] = make_ulonglong2(ct[2] ^ (jq == 2 ? e : 0ull), ct[3] ^ (jq == 3 ? e : 0ull));
+            }
+            if (lane == 0 && mk != NOKEY) atomicMin(kslot, mk);
+        };
+        if (tid < 3) S.keys[tid] = NOKEY;
+        __syncthreads();
+        publish(&S.keys[0], nb0);
+        __syncthreads();
+        int nnew = 0, kr = 0;  // kr: slot holding this iteration's key
+        for (;;) {
+            const unsigned kk = S.keys[kr];
+            if (kk == NOKEY || nb0 + nnew >= valid) break;
+            const int kn = kr == 2 ? 0 : kr + 1, kz = kn == 2 ? 0 : kn + 1;
+            if (tid == 0) S.keys[kz] = NOKEY;  // read last in the previous iteration
+            const int p = (int)(kk & 1023u), L = (int)(kk >> 10);
+            if (tid == p) {
+                used = true;
+                myj = nb0 + nnew;
+                key = NOKEY;
+                S.newslot[nnew] = p;
+                S.newlead[nnew] = L;
+                S.prow[myj] = row;
+            } else if (bit_of(cx, L)) {
+                const ulonglong2 *pv = reinterpret_cast<const ulonglong2 *>(S.cx[p]);
+                const ulonglong2 *pt = reinterpret_cast<const ulonglong2 *>(S.ct[p]);
+                const ulonglong2 v0 = pv[0], v1 = pv[1], t0 = pt[0], t1 = pt[1];
+                cx[0] ^= v0.x;
+                cx[1] ^= v0.y;
+                cx[2] ^= v1.x;
+                cx[3] ^= v1.y;
+                ct[0] ^= t0.x;
+                ct[1] ^= t0.y;
+                ct[2] ^= t1.x;
+                ct[3] ^= t1.y;
+                if (!used) key = any4(cx) ? ((unsigned)lead4(cx) << 10 | (unsigned)tid) : NOKEY;
+            }
+            ++nnew;
+            publish(&S.keys[kn], nb0 + nnew);
+            kr = kn;
+            __syncthreads();
+        }
+        __syncthreads();  // every key is read before the next chunk publishes
+        if (nnew == 0) continue;  // uniform
+        if (used) {
+            ct[0] ^= (myj >> 6) == 0 ? (1ull << (myj & 63)) : 0ull;
+            ct[1] ^= (myj >> 6) == 1 ? (1ull << (myj & 63)) : 0ull;
+            ct[2] ^= (myj >> 6) == 2 ? (1ull << (myj & 63)) : 0ull;
+            ct[3] ^= (myj >> 6) == 3 ? (1ull << (myj & 63)) : 0ull;
+#pragma unroll
+            for (int q = 0; q < WW; ++q) {
+                S.cx[tid][q] = cx[q];
+                S.ct[tid][q] = ct[q];
+            }
+        }
+        __syncthreads();
+        // older basis vectors: clear the new leading bits (the new vectors are
+        // reduced among themselves and zero at the older leads)
+        if (nb0 && tid < WBITS && ((S.have[tid >> 6] >> (tid & 63)) & 1)) {
+            u64 v[WW], t[WW];
+#pragma unroll
+            for (int q = 0; q < WW; ++q) {
+                v[q] = S.bd[tid][q];
+                t[q] = S.bt[tid][q];
+            }
+            const u64 ov[WW] = {v[0], v[1], v[2], v[3]};
+            for (int e = 0; e < nnew; ++e) {
+                if (bit_of(ov, S.newlead[e])) {
+                    xor4s(v, S.cx[S.newslot[e]]);
+                    xor4s(t, S.ct[S.newslot[e]]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < WW; ++q) {
+                S.bd[tid][q] = v[q];
+                S.bt[tid][q] = t[q];
+            }
+        }
+        __syncthreads();
+        if (tid < nnew) {
+            const int Ld = S.newlead[tid], sl = S.newslot[tid];
+#pragma unroll
+            for (int q = 0; q < WW; ++q) {
+                S.bd[Ld][q] = S.cx[sl][q];
+                S.bt[Ld][q] = S.ct[sl][q];
+            }
+        }
+        if (tid == 0) {
+            for (int e = 0; e < nnew; ++e) S.have[S.newlead[e] >> 6] |= 1ull << (S.newlead[e] & 63);
+            S.nb = nb0 + nnew;
+        }
+        __syncthreads();
+        if (S.nb < valid && base + WF_THREADS < na) {
+            // tables of the 16 combinations of basis vectors 4g..4g+3
+            for (int e = tid; e < 64 * 16; e += WF_THREADS) {
+                const int g = e >> 4, v = e & 15;
+                u64 a[WW] = {0, 0, 0, 0}, b[WW] = {0, 0, 0, 0};
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const int bb = 4 * g + h;
+                    if (((v >> h) & 1) && ((S.have[bb >> 6] >> (bb & 63)) & 1)) {
+                        xor4s(a, S.bd[bb]);
+                        xor4s(b, S.bt[bb]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < WW; ++q) {
+                    S.tab[g][v][q] = a[q];
+                    S.tabt[g][v][q] = b[q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // results: pivot t = t-th leading bit; P-index t is its physical row
+    const int nb = S.nb;
+    const long long r0 = ws->rank;
+    if (tid < WBITS && ((S.have[tid >> 6] >> (tid & 63)) & 1)) {
+        int t = 0;
+        for (int q = 0; q < (tid >> 6); ++q) t += __popcll(S.have[q]);
+        t += __popcll(S.have[tid >> 6] & ((1ull << (tid & 63)) - 1));
+#pragma unroll
+        for (int q = 0; q < WW; ++q) ws->tag[t][q] = S.bt[tid][q];
+        piv[r0 + t] = 64 * w + tid;
+    }
+    if (tid < nb) {
+        const int r = S.prow[tid];
+        ws->prow[tid] = r;
+        prow[r0 + tid] = r;
+        state[r] = 0;
+        stamp[r] = wid;
+    }
+    if (tid < WW) ws->have[tid] = S.have[tid];
+    if (tid == 0) S.cnt = walked;
+    __syncthreads();
+    // compact the walked part [0, walked) of the list to its right end, in
+    // order, dropping this window's pivot rows and rows known to be zero from
+    // the window on; chunks go from the last to the first, so every write lands
+    // at or after the chunk being read
+    for (int c0 = ((walked - 1) / WF_THREADS) * WF_THREADS; walked > 0 && c0 >= 0; c0 -= WF_THREADS) {
+        const int k = c0 + tid;
+        int row = -1;
+        if (k < walked) row = L0[k];
+        const bool keep = row >= 0 && state[row] && live[row];
+        int total;
+        const int slot = block_slot(keep, S.wsum, total);
+        const int wpos = S.cnt - total;
+        if (keep) L0[wpos + slot] = row;
+        __syncthreads();
+        if (tid == 0) S.cnt = wpos;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        ws->rt = nb;
+        ws->nu = 0;
+        ws->lbase += S.cnt;  // S.cnt = entries dropped
+        ws->na = na - S.cnt;
+        ws->rank = r0 + nb;
+    }
+}
+
+// ---------------------------------------------------------------- window_combine
+// Block: CB_W words x every pivot.  R_t = XOR_j T[t][j] A[P_j] is evaluated
+// four P-indices at a time from 64 tables of the 16 combinations of P rows
+// 4g..4g+3 (restricted to the block's words).
+namespace {
+constexpr int CB_W = 4;
+struct CbSmem {
+    u64 tab[64][16][CB_W];  // 32 KB
+    u64 rows[WBITS][CB_W];  // the P rows' words
+    u64 tag[WBITS][WW];
+};
+}
+
+__global__ void __launch_bounds__(256)
+window_combine_kernel(const u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const WinState *ws,
+                      u64 *__restrict__ Rbuf, i64 ldr)
+{
+    extern __shared__ __align__(16) unsigned char cb_raw[];
+    CbSmem &S = *reinterpret_cast<CbSmem *>(cb_raw);
+    const int rt = ws->rt;
+    if (rt == 0) return;
+    const int tid = threadIdx.x;
+    const i64 w0 = w + (i64)blockIdx.x * CB_W;
+    {
+        const int j = tid;  // 256 threads: one P row each
+        u64 v[CB_W];
+        if (j < rt) {
+            const u64 *src = M + (i64)ws->prow[j] * ld + w0;
+#pragma unroll
+            for (int q = 0; q < CB_W; ++q) v[q] = (w0 + q < wc) ? src[q] : 0ull;
+        } else {
+#pragma unroll
+            for (int q = 0; q < CB_W; ++q) v[q] = 0;
+        }
+#pragma unroll
+        for (int q = 0; q < CB_W; ++q) S.rows[j][q] = v[q];
+#pragma unroll
+        for (int q = 0; q < WW; ++q) S.tag[j][q] = j < rt ? ws->tag[j][q] : 0ull;
+    }
+    __syncthreads();
+    for (int e = tid; e < 64 * 16; e += 256) {
+        const int g = e >> 4, v = e & 15;
+        u64 a[CB_W] = {};
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+            if ((v >> h) & 1) {
+#pragma unroll
+                for (int q = 0; q < CB_W; ++q) a[q] ^= S.rows[4 * g + h][q];
+            }
+#pragma unroll
+        for (int q = 0; q < CB_W; ++q) S.tab[g][v][q] = a[q];
+    }
+    __syncthreads();
+    // thread: word q = tid % CB_W, pivots t = tid / CB_W + 64 i
+    const int q = tid % CB_W;
+    for (int t = tid / CB_W; t < rt; t += 256 / CB_W) {
+        u64 acc = 0;
+#pragma unroll
+        for (int qq = 0; qq < WW; ++qq) {
+            const u64 tg = S.tag[t][qq];
+#pragma unroll
+            for (int g = 0; g < 16; ++g) acc ^= S.tab[16 * qq + g][(tg >> (4 * g)) & 15][q];
+        }
+        if (w0 + q < wc) Rbuf[(i64)t * ldr + (w0 + q - w)] = acc;
+    }
+}
+
+// ---------------------------------------------------------------- window_coef
+// 4 bits -> 4 bytes of 0/1.
+__device__ __forceinline__ u32 nib_bytes(u32 v) { return ((v & 15u) * 0x00204081u) & 0x01010101u; }
+
+// Rows to update: rank form, the list of active rows (pivot rows of this
+// window already removed); RREF form, every row except this window's pivots.
+__global__ void __launch_bounds__(256)
+window_coef_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const int *__restrict__ list,
+                   const int *stamp, int wid, int rref, WinState *ws, int *ulist, unsigned char *X8,
+                   unsigned char *live)
+{
+    if (ws->rt == 0) return;
+    u64 hv[WW];
+#pragma unroll
+    for (int q = 0; q < WW; ++q) hv[q] = ws->have[q];
+    const i64 cnt = rref ? m : (i64)ws->na;
+    list += ws->lbase;
+    const int wn = (wc - w) < WW ? (int)(wc - w) : WW;
+    const int lane = threadIdx.x & 31;
+    const i64 stride = (i64)gridDim.x * blockDim.x;
+    for (i64 i0 = (i64)blockIdx.x * blockDim.x; i0 < cnt; i0 += stride) {
+        const i64 idx = i0 + threadIdx.x;
+        i64 row = -1;
+        if (idx < cnt) {
+            row = rref ? idx : (i64)list[idx];
+            if (rref && stamp[row] == wid) row = -1;
+        }
+        u64 xc[WW] = {0, 0, 0, 0};
+        if (row >= 0) {
+            int pos = 0;
+#pragma unroll
+            for (int q = 0; q < WW; ++q) {
+                const u64 h = hv[q];
+                if (q >= wn || !h) continue;
+                const u64 x = M[row * ld + w + q];
+                u64 e;
+                int c;
+                if (h == ~0ull) {
+                    e = x;
+                    c = 64;
+                } else {
+                    e = 0;
+                    c = 0;
+                    u64 hh = h;
+                    while (hh) {
+                        const u64 lb = hh & (~hh + 1);
+                        if (x & lb) e |= 1ull << c;
+                        ++c;
+                        hh ^= lb;
+                    }
+                }
+                const int wq = pos >> 6, sb = pos & 63;
+                or_word(xc, wq, e << sb);
+                if (sb && sb + c > 64) or_word(xc, wq + 1, e >> (64 - sb));
+                pos += c;
+            }
+        }
+        const bool nz = any4(xc);
+        const unsigned b = __ballot_sync(0xffffffffu, nz);
+        int basepos = 0;
+        if (b) {
+            if (lane == 0) basepos = atomicAdd(&ws->nu, __popc(b));
+            basepos = __shfl_sync(0xffffffffu, basepos, 0);
+        }
+        if (nz) {
+            const int slot = basepos + __popc(b & ((1u << lane) - 1));
+            ulist[slot] = (int)row;
+            live[row] = 0;  // set again by the update if the row stays nonzero
+            uint4 *dst = reinterpret_cast<uint4 *>(X8 + (size_t)slot * WBITS);
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const u32 bits = (u32)(xc[c >> 2] >> (16 * (c & 3))) & 0xFFFFu;
+                dst[c] = make_uint4(nib_bytes(bits), nib_bytes(bits >> 4), nib_bytes(bits >> 8), nib_bytes(bits >> 12));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- window_rt
+// Block W (word w + W): Rt8 rows 64W..64W+63 and word w + W of every row P_t.
+__global__ void __launch_bounds__(256)
+window_rt_kernel(u64 *__restrict__ M, i64 ld, i64 w, const u64 *__restrict__ Rbuf, i64 ldr, const WinState *ws,
+                 unsigned char *Rt8)
+{
+    __shared__ u64 col[WBITS];
+    const int rt = ws->rt;
+    if (rt == 0) return;
+    const int tid = threadIdx.x;
+    const i64 W = blockIdx.x;
+    const u64 v = tid < rt ? Rbuf[(i64)tid * ldr + W] : 0ull;
+    col[tid] = v;
+    if (tid < rt) M[(i64)ws->prow[tid] * ld + w + W] = v;
+    __syncthreads();
+    for (int e = tid; e < 64 * 16; e += 256) {
+        const int jl = e >> 4, c = e & 15;
+        u32 o[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            u32 x = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) x |= (u32)((col[16 * c + 4 * r + b] >> jl) & 1) << (8 * b);
+            o[r] = x;
+        }
+        *reinterpret_cast<uint4 *>(Rt8 + ((size_t)(W * 64 + jl)) * WBITS + 16 * c) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// ---------------------------------------------------------------- tc_update
+namespace {
+constexpr int UM = 128, UN = 256;             // output tile
+constexpr int UBOX = 128;                     // K bytes per TMA box (128-byte swizzle)
+constexpr int UA_BOX = UM * UBOX;             // 16 KB
+constexpr int UB_BOX = UN * UBOX;             // 32 KB
+constexpr int UA_BYTES = 2 * UA_BOX;          // K = 256
+constexpr int UB_BYTES = 2 * UB_BOX;
+constexpr int U_STAGES = 4;                   // X8 tiles in flight
+constexpr int U_BSTAGES = 1;                  // Rt8 strips in shared memory
+constexpr int U_SMEM = U_BSTAGES * UB_BYTES + U_STAGES * UA_BYTES + 1024 + 256;
+constexpr int U_MCH = 8;                      // row tiles per work unit
+constexpr int U_EPI_THREADS = 128;
+
+struct UCtl {
+    u64 bfull[U_BSTAGES], bempty[U_BSTAGES];
+    u64 afull[U_STAGES], aempty[U_STAGES];
+    u64 accfull[2], accempty[2];
+    u64 drain;
+    u32 tmem;
+    int abort;
+};
+
+// bit `pos` of base := bit 0 of src
+__device__ __forceinline__ u32 bfi1(u32 src, u32 base, u32 pos)
+{
+    u32 d;
+    asm("bfi.b32 %0, %1, %2, %3, 1;" : "=r"(d) : "r"(src), "r"(base), "r"(pos));
+    return d;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(192, 1)
+tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmR,
+                 u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const WinState *ws, const int *__restrict__ ulist,
+                 unsigned char *live, u32 *err)
+{
+    const int rt = ws->rt, nu = ws->nu;
+    if (rt == 0 || nu == 0) return;
+    const i64 lw = wc - w;
+    const int strips = (int)((lw + 3) / 4);
+    const int mt = (nu + UM - 1) / UM;
+    const int chunks = (mt + U_MCH - 1) / U_MCH;
+    const long long units = (long long)strips * chunks;
+    const long long ub = units * blockIdx.x / gridDim.x, ue = units * (blockIdx.x + 1) / gridDim.x;
+    if (ub >= ue) return;
+
+    extern __shared__ unsigned char u_raw[];
+    unsigned char *smem =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(u_raw) + 1023) & ~(uintptr_t)1023);
+    unsigned char *sB = smem;
+    unsigned char *sA = smem + U_BSTAGES * UB_BYTES;
+    UCtl *ctl = reinterpret_cast<UCtl *>(sA + U_STAGES * UA_BYTES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < U_BSTAGES; ++s) {
+            ptx::mbar_init(&ctl->bfull[s], 1);
+            ptx::mbar_init(&ctl->bempty[s], 1);
+        }
+        for (int s = 0; s < U_STAGES; ++s) {
+            ptx::mbar_init(&ctl->afull[s], 1);
+            ptx::mbar_init(&ctl->aempty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            ptx::mbar_init(&ctl->accfull[a], 1);
+            ptx::mbar_init(&ctl->accempty[a], U_EPI_THREADS);
+        }
+        ptx::mbar_init(&ctl->drain, 1);
+        ctl->abort = 0;
+        ptx::fence_barrier_init();
+    }
+    if (warp == 0 && lane == 0) {
+        ptx::prefetch_tmap(&tmX);
+        ptx::prefetch_tmap(&tmR);
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc(&ctl->tmem, 512);
+        ptx::tmem_relinquish();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const u32 tmem = ctl->tmem;
+    volatile int *abort_flag = &ctl->abort;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // strip loads (nbl) and tile loads (it) in the order the MMA warp consumes them
+            int nbl = 0, it = 0, prev_strip = -1;
+            int last_a[U_STAGES], last_b[U_BSTAGES];
+#pragma unroll
+            for (int q = 0; q < U_STAGES; ++q) last_a[q] = -1;
+#pragma unroll
+            for (int q = 0; q < U_BSTAGES; ++q) last_b[q] = -1;
+            bool ok = true;
+            for (long long u = ub; u < ue && ok; ++u) {
+                const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+                if (strip != prev_strip) {
+                    const int bs = nbl % U_BSTAGES;
+                    if (nbl >= U_BSTAGES && !ptx::mbar_wait(&ctl->bempty[bs], ((nbl / U_BSTAGES) - 1) & 1, err)) {
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *b = sB + bs * UB_BYTES;
+                    ptx::mbar_arrive_expect_tx(&ctl->bfull[bs], UB_BYTES);
+                    ptx::tma_load_2d(b, &tmR, &ctl->bfull[bs], 0, strip * UN);
+                    ptx::tma_load_2d(b + UB_BOX, &tmR, &ctl->bfull[bs], UBOX, strip * UN);
+                    last_b[bs] = nbl / U_BSTAGES;
+                    ++nbl;
+                    prev_strip = strip;
+                }
+                const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
+                for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+                    const int s = it % U_STAGES;
+                    if (it >= U_STAGES && !ptx::mbar_wait(&ctl->aempty[s], ((it / U_STAGES) - 1) & 1, err)) {
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *a = sA + s * UA_BYTES;
+                    ptx::mbar_arrive_expect_tx(&ctl->afull[s], UA_BYTES);
+                    ptx::tma_load_2d(a, &tmX, &ctl->afull[s], 0, tile * UM);
+                    ptx::tma_load_2d(a + UA_BOX, &tmX, &ctl->afull[s], UBOX, tile * UM);
+                    last_a[s] = it / U_STAGES;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                // let every issued copy land before the CTA's shared memory goes away
+                for (int s = 0; s < U_BSTAGES; ++s)
+                    if (last_b[s] >= 0) ptx::mbar_wait(&ctl->bfull[s], last_b[s] & 1, nullptr);
+                for (int s = 0; s < U_STAGES; ++s)
+                    if (last_a[s] >= 0) ptx::mbar_wait(&ctl->afull[s], last_a[s] & 1, nullptr);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr u32 idesc = ptx::idesc_i8(UM, UN);
+            int nbl = 0, it = 0, prev_strip = -1, bs = 0;
+            bool ok = true;
+            for (long long u = ub; u < ue && ok; ++u) {
+                const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+                if (strip != prev_strip) {
+                    bs = nbl % U_BSTAGES;
+                    if (!ptx::mbar_wait(&ctl->bfull[bs], (nbl / U_BSTAGES) & 1, err) || *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    ++nbl;
+                    prev_strip = strip;
+                }
+                const u32 b0 = ptx::smem_u32(sB + bs * UB_BYTES);
+                const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
+                for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+                    const int s = it % U_STAGES, acc = it & 1;
+                    if (!ptx::mbar_wait(&ctl->afull[s], (it / U_STAGES) & 1, err) ||
+                        (it >= 2 && !ptx::mbar_wait(&ctl->accempty[acc], ((it >> 1) - 1) & 1, err)) ||
+                        *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const u32 a0 = ptx::smem_u32(sA + s * UA_BYTES);
+                    const u32 d = tmem + (u32)(acc * UN);
+#pragma unroll
+                    for (int kb = 0; kb < 2; ++kb)
+#pragma unroll
+                        for (int kk = 0; kk < UBOX / 32; ++kk)
+                            ptx::umma_i8(d, ptx::desc_k_sw128(a0 + kb * UA_BOX + kk * 32),
+                                         ptx::desc_k_sw128(b0 + kb * UB_BOX + kk * 32), idesc, (kb | kk) != 0);
+                    ptx::umma_commit(&ctl->aempty[s]);
+                    ptx::umma_commit(&ctl->accfull[acc]);
+                }
+                if (!ok) break;
+                // the strip's buffer is free once this unit's products are done
+                const bool next_same = (u + 1 < ue) && ((int)((u + 1) / chunks) == strip);
+                if (!next_same) ptx::umma_commit(&ctl->bempty[bs]);
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                ptx::umma_commit(&ctl->drain);
+                ptx::mbar_wait(&ctl->drain, 0, nullptr);
+            }
+        }
+        __syncwarp();
+    } else {
+        const int ew = warp & 3;  // TMEM lane quarter of this warp
+        int it = 0;
+        bool ok = true;
+        for (long long u = ub; u < ue && ok; ++u) {
+            const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+            const i64 w0 = w + (i64)strip * 4;
+            const int nw = (wc - w0) < 4 ? (int)(wc - w0) : 4;
+            const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
+            for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+                const int acc = it & 1;
+                // the row's current words are fetched while the product is computed
+                const int slot = tile * UM + ew * 32 + lane;
+                u64 *dst = nullptr;
+                int urow = 0;
+                u64 old[4] = {0, 0, 0, 0};
+                if (slot < nu) {
+                    urow = ulist[slot];
+                    dst = M + (i64)urow * ld + w0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (q < nw) old[q] = dst[q];
+                }
+                if (!ptx::mbar_wait(&ctl->accfull[acc], (it >> 1) & 1, err) || *abort_flag) {
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                u32 bits[UN / 32];
+                {
+                    // two 32-column buffers: the load of chunk c+1 is in flight
+                    // while chunk c is reduced to its parity bits
+                    const u32 tbase = tmem + ((u32)(ew * 32) << 16) + (u32)(acc * UN);
+                    u32 ra[32], rb[32];
+                    ptx::tmem_ld_32x32b_x32(tbase, ra);
+                    ptx::tmem_ld_wait();
+#pragma unroll
+                    for (int c = 0; c < UN / 32; c += 2) {
+                        ptx::tmem_ld_32x32b_x32(tbase + (u32)((c + 1) * 32), rb);
+                        u32 b = ra[0] & 1u;
+#pragma unroll
+                        for (int j = 1; j < 32; ++j) b = bfi1(ra[j], b, (u32)j);
+                        bits[c] = b;
+                        ptx::tmem_ld_wait();
+                        if (c + 2 < UN / 32) ptx::tmem_ld_32x32b_x32(tbase + (u32)((c + 2) * 32), ra);
+                        b = rb[0] & 1u;
+#pragma unroll
+                        for (int j = 1; j < 32; ++j) b = bfi1(rb[j], b, (u32)j);
+                        bits[c + 1] = b;
+                        if (c + 2 < UN / 32) ptx::tmem_ld_wait();
+                    }
+                }
+                ptx::tc_fence_before();
+                ptx::mbar_arrive(&ctl->accempty[acc]);
+                if (dst) {
+                    u64 any = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (q < nw) {
+                            const u64 v = old[q] ^ ((u64)bits[2 * q] | ((u64)bits[2 * q + 1] << 32));
+                            dst[q] = v;
+                            any |= v;
+                        }
+                    }
+                    if (any) live[urow] = 1;
+                }
+            }
+        }
+        if (!ok) *abort_flag = 1;
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc(tmem, 512);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The first window's list: every row, in order.
+__global__ void list_init_kernel(int *list, i64 m, WinState *ws)
+{
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x)
+        list[i] = (int)i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ws->na = (int)m;
+        ws->lbase = 0;
+    }
+}
+
+static int grid_for(i64 total)
+{
+    i64 g = (total + 255) / 256;
+    const i64 cap = (i64)sm_count() * 8;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+namespace {
+struct TcLayout {
+    size_t state, stamp, live, ws, ulist, list, x8, rt8, rbuf, total;
+    i64 mpad, npad;
+};
+
+TcLayout tc_layout(i64 m, i64 n)
+{
+    TcLayout L{};
+    const i64 wc = words_of(n);
+    L.mpad = (m + UM - 1) / UM * UM;
+    L.npad = (64 * wc + UN - 1) / UN * UN;
+    size_t off = 0;
+    L.state = off;  off += al256((size_t)m);
+    L.stamp = off;  off += al256((size_t)m * 4);
+    L.live = off;   off += al256((size_t)m);
+    L.ws = off;     off += al256(sizeof(WinState));
+    L.ulist = off;  off += al256((size_t)m * 4);
+    L.list = off;   off += al256((size_t)m * 4);
+    L.x8 = off;     off += al256((size_t)L.mpad * WBITS);
+    L.rt8 = off;    off += al256((size_t)L.npad * WBITS);
+    L.rbuf = off;   off += al256((size_t)WBITS * (size_t)wc * 8);
+    L.total = off;
+    return L;
+}
+}  // namespace
+
+size_t elim_tc_workspace(i64 m, i64 n) { return tc_layout(m, n).total; }
+
+mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank, long long *d_piv,
+                           long long *d_prow, void *wsp, size_t ws_bytes, cudaStream_t s)
+{
+    const TcLayout L = tc_layout(m, n);
+    if (!wsp || ws_bytes < L.total) {
+        set_error("elimination workspace of %zu bytes needed, %zu given", L.total, ws_bytes);
+        return MELA_ERR_INVALID;
+    }
+    if (L.mpad / UM > INT_MAX / 2 || L.npad > ((i64)1 << 31)) {
+        set_error("tensor-core elimination: matrix too large");
+        return MELA_ERR_UNSUPPORTED;
+    }
+    unsigned char *b = (unsigned char *)wsp;
+    unsigned char *state = b + L.state;
+    int *stamp = (int *)(b + L.stamp);
+    WinState *ws = (WinState *)(b + L.ws);
+    int *ulist = (int *)(b + L.ulist);
+    unsigned char *X8 = b + L.x8;
+    unsigned char *Rt8 = b + L.rt8;
+    u64 *Rbuf = (u64 *)(b + L.rbuf);
+    int *list = (int *)(b + L.list);
+    unsigned char *live = b + L.live;
+    const i64 wc = words_of(n);
+
+    CUtensorMap mx, mr;
+    mela_status st = make_u8_kmajor_map(&mx, X8, L.mpad, WBITS, UM);
+    if (st != MELA_OK) return st;
+    st = make_u8_kmajor_map(&mr, Rt8, L.npad, WBITS, UN);
+    if (st != MELA_OK) return st;
+
+    MELA_CUDA_TRY(cudaMemsetAsync(state, 1, (size_t)m, s));
+    MELA_CUDA_TRY(cudaMemsetAsync(stamp, 0xff, (size_t)m * 4, s));
+    MELA_CUDA_TRY(cudaMemsetAsync(live, 1, (size_t)m, s));
+    MELA_CUDA_TRY(cudaMemsetAsync(ws, 0, sizeof(WinState), s));
+    list_init_kernel<<<grid_for(m), 256, 0, s>>>(list, m, ws);
+    const size_t wf_smem = sizeof(WfSmem);
+    MELA_CUDA_TRY(cudaFuncSetAttribute(window_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)wf_smem));
+    MELA_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, U_SMEM));
+    const int cb_smem = (int)sizeof(CbSmem);
+    MELA_CUDA_TRY(cudaFuncSetAttribute(window_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cb_smem));
+    const int sms = sm_count();
+    const i64 coef_blocks_full = (m + 255) / 256;
+    const int coef_blocks = (int)(coef_blocks_full < (i64)sms * 8 ? coef_blocks_full : (i64)sms * 8);
+    u32 *err = device_error_word();
+    int wid = 0;
+    for (i64 w = 0; w < wc; w += WW, ++wid) {
+        const i64 lw = wc - w;
+        window_factor_kernel<<<1, WF_THREADS, wf_smem, s>>>(M, ld, m, n, w, list, live, state, stamp, wid, ws, d_piv,
+                                                            d_prow);
+        window_combine_kernel<<<(unsigned)((lw + CB_W - 1) / CB_W), 256, cb_smem, s>>>(
+            M, ld, wc, w, ws, Rbuf, wc);
+        window_coef_kernel<<<coef_blocks, 256, 0, s>>>(M, ld, m, wc, w, list, stamp, wid, rref, ws, ulist, X8, live);
+        window_rt_kernel<<<(unsigned)lw, 256, 0, s>>>(M, ld, w, Rbuf, wc, ws, Rt8);
+        const i64 strips = (lw + 3) / 4;
+        const i64 units_max = strips * ((L.mpad / UM + U_MCH - 1) / U_MCH);
+        const int grid = (int)(units_max < sms ? units_max : sms);
+        tc_update_kernel<<<grid, 192, U_SMEM, s>>>(mx, mr, M, ld, wc, w, ws, ulist, live, err);
+    }
+    MELA_LAUNCH_CHECK("tensor-core elimination");
+    MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &ws->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    return MELA_OK;
+}
+
+}  // namespace mela

@@ -254,6 +254,11 @@ static mela_status make_map(CUtensorMap *map, const unsigned char *base, i64 row
     return MELA_OK;
 }
 
+mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 rows, i64 kp, int box_rows)
+{
+    return make_map(map, base, rows, kp, box_rows);
+}
+
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
                            i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4)
 {

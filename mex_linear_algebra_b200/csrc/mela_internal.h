@@ -1,6 +1,8 @@
 // mela_internal.h -- launchers shared between the library's translation units.
 #pragma once
 
+#include <cuda.h>
+
 #include "mela_common.cuh"
 
 namespace mela {
@@ -31,6 +33,9 @@ mela_status launch_gemm_plain(const u64 *A, i64 lda, const u64 *Bt, i64 ldbt, u6
 // fp4 = true: packed e2m1 operands (kp counts bytes, two values each), kind::mxf4.
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
                            i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4);
+// TMA map of a K-major byte matrix rows x kp (row pitch kp bytes): boxes of
+// 128 bytes x box_rows rows with 128-byte swizzle, as the tcgen05 kernels read them.
+mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 rows, i64 kp, int box_rows);
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                              i64 m, i64 k, i64 n, cudaStream_t s);
 

@@ -44,15 +44,27 @@ def test_dense_rank_and_null_full_size(cuda):
     dr = torch.zeros(1, dtype=torch.int64, device="cuda")
     dpv = torch.empty(m, dtype=torch.int64, device="cuda")
     dpr = torch.empty(m, dtype=torch.int64, device="cuda")
-    for form in ("m4ri", "m4ri_k4", "plain"):
+    for form in ("m4ri", "m4ri_k4", "plain", "tc"):
         Mx = A.clone()
         _lib.check(L.mela_dev_rank(_lib.ELIM_VARIANTS[form], Mx.data_ptr(), wc, m, n, dr.data_ptr(),
                                    dpv.data_ptr(), dpr.data_ptr(), ws.data_ptr(), wsb, s))
         assert int(dr.item()) == golden["rank"], form
+    # RREF by the tensor-core form equals the blocked form's (pivots and rows)
+    Mt = A.clone()
+    _lib.check(L.mela_dev_rref(_lib.ELIM_TC, Mt.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                               dpr.data_ptr(), ws.data_ptr(), wsb, s))
+    rt = int(dr.item())
+    piv_t = dpv[:rt].clone()
+    rows_t = Mt[dpr[:rt]].clone()
+    del Mt
     Mx = A.clone()
     _lib.check(L.mela_dev_rref(_lib.ELIM_M4RI, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
                                dpr.data_ptr(), ws.data_ptr(), wsb, s))
     r = int(dr.item())
+    assert rt == r
+    assert torch.equal(piv_t, dpv[:r])
+    assert torch.equal(rows_t, Mx[dpr[:r]])
+    del rows_t
     f = n - r
     Zt = torch.empty((f, wc), dtype=torch.int64, device="cuda")
     nwb = L.mela_null_workspace_size(n, r)

@@ -1,6 +1,7 @@
 """Rank, RREF and null space on the GPU against the oracle (bit-exact).
 
-Both elimination forms (plain per-pivot, blocked Four-Russians) must give the
+Every elimination form (plain per-pivot, blocked Four-Russians with 8- and
+4-bit tables, single-CTA fused, tensor-core trailing update) must give the
 reference's rank, its greedy pivot columns, its RREF rows and its null-space
 basis.  Shapes cover word boundaries, tall and wide matrices, several
 selection chunks (m > 1024), several update row tiles (m > 1024) and column
@@ -15,7 +16,7 @@ from gpu_util import to_dev, to_host, valid_words
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ("plain", "m4ri", "m4ri_k4", "fused")
+FORMS = ("plain", "m4ri", "m4ri_k4", "fused", "tc")
 
 
 def dev_rref(P, m, n, form, rref=True):
@@ -132,3 +133,31 @@ def test_forms_agree_large(cuda):
         _, r, piv, _ = dev_rref(Ah, m, n, form, rref=False)
         assert r == want
     torch.cuda.synchronize()
+
+
+def _rref_rows(M, m, n, r, prow):
+    rows = to_host(M)[prow]
+    return valid_words(rows, n)
+
+
+@pytest.mark.parametrize("shape,rank", [((3000, 2600), None), ((2600, 3000), 1900), ((1500, 9000), None),
+                                        ((5000, 700), 300)])
+def test_tc_rref_matches_blocked(cuda, shape, rank):
+    """The tensor-core form against the 8-bit blocked form: dense windows that
+    fill after a few hundred rows, several scan chunks and update tiles, and
+    low-rank inputs whose later windows hold no pivot."""
+    from mex_linear_algebra_b200 import device as D
+    m, n = shape
+    if rank is None:
+        P = O.rand_dense(41, m + n, m, n)
+    else:
+        L = D.rand_dense(43, 0, m, rank)
+        R = D.rand_dense(43, 1, rank, n)
+        P = to_host(D.matmul(L, R, m, rank, n, variant="plain"))
+    for rref in (False, True):
+        Ma, ra, pa, qa = dev_rref(P, m, n, "m4ri", rref=rref)
+        Mb, rb, pb, qb = dev_rref(P, m, n, "tc", rref=rref)
+        assert ra == rb
+        assert np.array_equal(pa, pb)
+        if rref:
+            assert np.array_equal(_rref_rows(Ma, m, n, ra, qa), _rref_rows(Mb, m, n, rb, qb))
