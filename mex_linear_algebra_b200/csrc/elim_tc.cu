@@ -103,6 +103,7 @@ __device__ __forceinline__ void xor4s(u64 (&a)[WW], const u64 *b)
     for (int q = 0; q < WW; ++q) a[q] ^= b[q];
 }
 __device__ __forceinline__ bool any4(const u64 (&v)[WW]) { return (v[0] | v[1] | v[2] | v[3]) != 0; }
+
 __device__ __forceinline__ int lead4(const u64 (&v)[WW])
 {
     return v[0] ? ctz64w(v[0]) : (v[1] ? 64 + ctz64w(v[1]) : (v[2] ? 128 + ctz64w(v[2]) : 192 + ctz64w(v[3])));
@@ -561,9 +562,19 @@ constexpr int UA_BYTES = 2 * UA_BOX;          // K = 256
 constexpr int UB_BYTES = 2 * UB_BOX;
 constexpr int U_STAGES = 4;                   // X8 tiles in flight
 constexpr int U_BSTAGES = 1;                  // Rt8 strips in shared memory
-constexpr int U_SMEM = U_BSTAGES * UB_BYTES + U_STAGES * UA_BYTES + 1024 + 256;
+constexpr int U_STAGE_BYTES = 2 * 2 * UM * 4 * 8;  // per accumulator, two 128-row x 4-word stages
+constexpr int U_SMEM = U_BSTAGES * UB_BYTES + U_STAGES * UA_BYTES + U_STAGE_BYTES + 1024 + 256;
 constexpr int U_MCH = 8;                      // row tiles per work unit
-constexpr int U_EPI_THREADS = 128;
+constexpr int U_EPI_THREADS = 256;           // warps draining one accumulator: 2 per TMEM lane quarter
+constexpr int U_THREADS = 64 + 2 * U_EPI_THREADS;  // and the same for the other accumulator
+
+// bit `pos` of base := bit 0 of src
+__device__ __forceinline__ u32 bfi1(u32 src, u32 base, u32 pos)
+{
+    u32 d;
+    asm("bfi.b32 %0, %1, %2, %3, 1;" : "=r"(d) : "r"(src), "r"(base), "r"(pos));
+    return d;
+}
 
 struct UCtl {
     u64 bfull[U_BSTAGES], bempty[U_BSTAGES];
@@ -574,16 +585,9 @@ struct UCtl {
     int abort;
 };
 
-// bit `pos` of base := bit 0 of src
-__device__ __forceinline__ u32 bfi1(u32 src, u32 base, u32 pos)
-{
-    u32 d;
-    asm("bfi.b32 %0, %1, %2, %3, 1;" : "=r"(d) : "r"(src), "r"(base), "r"(pos));
-    return d;
-}
 }  // namespace
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(U_THREADS, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmR,
                  u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const WinState *ws, const int *__restrict__ ulist,
                  unsigned char *live, u32 *err)
@@ -603,7 +607,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(u_raw) + 1023) & ~(uintptr_t)1023);
     unsigned char *sB = smem;
     unsigned char *sA = smem + U_BSTAGES * UB_BYTES;
-    UCtl *ctl = reinterpret_cast<UCtl *>(sA + U_STAGES * UA_BYTES);
+    u64 *stage = reinterpret_cast<u64 *>(sA + U_STAGES * UA_BYTES);  // [acc][2][UM][4]
+    UCtl *ctl = reinterpret_cast<UCtl *>(sA + U_STAGES * UA_BYTES + U_STAGE_BYTES);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
@@ -745,73 +750,108 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
         }
         __syncwarp();
     } else {
-        const int ew = warp & 3;  // TMEM lane quarter of this warp
-        int it = 0;
+        // Sixteen warps: for each of the two accumulators (tiles with
+        // it % 2 == g), two warps per TMEM lane quarter, one per 128-column
+        // half.  A tile's packed parity words go through shared memory, so
+        // that the read-modify-write of the rows is done with 32 contiguous
+        // bytes per row (4 lanes a row, 8 rows a warp instruction).  The
+        // rows' current words for a tile are fetched before the previous
+        // tile is drained.
+        const int e = warp - 2;
+        const int ew = warp & 3;          // TMEM lane quarter of this warp
+        const int g = (e >> 2) & 1;       // accumulator
+        const int half = e >> 3;          // columns 128*half .. +127 (words 2*half, 2*half+1)
+        const int gt = ((e >> 3) << 7) | ((e & 3) << 5) | lane;  // 0..255 within the group
+        u64 *gstage = stage + (size_t)g * 2 * UM * 4;
+        int it = 0, k = 0;
         bool ok = true;
-        for (long long u = ub; u < ue && ok; ++u) {
+        // previous own tile
+        int p_it = 0;
+        i64 p_w0 = 0;
+        int p_nw = 0;
+        int p_row[2] = {-1, -1};
+        u64 p_old[2] = {0, 0};
+        // Every warp of the group reaches the group barrier once per tile, on
+        // the error path too (a failed wait skips the work, not the barrier).
+        auto drain_and_write = [&]() -> bool {
+            const int acc = p_it & 1;
+            const bool good = !*abort_flag && ptx::mbar_wait(&ctl->accfull[acc], (p_it >> 1) & 1, err);
+            if (!good) *abort_flag = 1;
+            u32 pb0 = 0, pb1 = 0, pb2 = 0, pb3 = 0;
+            if (good) {
+                ptx::tc_fence_after();
+                const u32 tbase = tmem + ((u32)(ew * 32) << 16) + (u32)(acc * UN + half * 128);
+#pragma unroll 1
+                for (int h = 0; h < 4; ++h) {
+                    u32 r[32];
+                    ptx::tmem_ld_32x32b_x32(tbase + (u32)(h * 32), r);
+                    ptx::tmem_ld_wait();
+                    u32 b = r[0] & 1u;
+#pragma unroll
+                    for (int j = 1; j < 32; ++j) b = bfi1(r[j], b, (u32)j);
+                    pb0 = h == 0 ? b : pb0;
+                    pb1 = h == 1 ? b : pb1;
+                    pb2 = h == 2 ? b : pb2;
+                    pb3 = h == 3 ? b : pb3;
+                }
+                ptx::tc_fence_before();
+                ptx::mbar_arrive(&ctl->accempty[acc]);
+            }
+            // stage row (ew*32 + lane), words 2*half, 2*half+1
+            u64 *st = gstage + (size_t)((k - 1) & 1) * UM * 4 + (size_t)(ew * 32 + lane) * 4 + 2 * half;
+            *reinterpret_cast<ulonglong2 *>(st) =
+                make_ulonglong2((u64)pb0 | ((u64)pb1 << 32), (u64)pb2 | ((u64)pb3 << 32));
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(U_EPI_THREADS) : "memory");
+            // items gt and gt + 256: row = item / 4, word = item % 4
+            const u64 *sb = gstage + (size_t)((k - 1) & 1) * UM * 4;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int item = gt + 256 * c;
+                const int q = item & 3;
+                u64 v = 0;
+                if (good && p_row[c] >= 0 && q < p_nw) {
+                    v = p_old[c] ^ sb[item];
+                    M[(i64)p_row[c] * ld + p_w0 + q] = v;
+                }
+                // one flag per row: the four lanes of a row combine their words
+                v |= __shfl_xor_sync(0xffffffffu, v, 1);
+                v |= __shfl_xor_sync(0xffffffffu, v, 2);
+                if (q == 0 && p_row[c] >= 0 && v) live[p_row[c]] = 1;
+            }
+            return good;
+        };
+        for (long long u = ub; u < ue; ++u) {
             const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
             const i64 w0 = w + (i64)strip * 4;
             const int nw = (wc - w0) < 4 ? (int)(wc - w0) : 4;
             const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
             for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
-                const int acc = it & 1;
-                // the row's current words are fetched while the product is computed
-                const int slot = tile * UM + ew * 32 + lane;
-                u64 *dst = nullptr;
-                int urow = 0;
-                u64 old[4] = {0, 0, 0, 0};
-                if (slot < nu) {
-                    urow = ulist[slot];
-                    dst = M + (i64)urow * ld + w0;
+                if ((it & 1) != g) continue;
+                // fetch this tile's words (coalesced layout), then finish the previous tile
+                int row[2] = {-1, -1};
+                u64 old[2] = {0, 0};
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (q < nw) old[q] = dst[q];
-                }
-                if (!ptx::mbar_wait(&ctl->accfull[acc], (it >> 1) & 1, err) || *abort_flag) {
-                    ok = false;
-                    break;
-                }
-                ptx::tc_fence_after();
-                u32 bits[UN / 32];
-                {
-                    // two 32-column buffers: the load of chunk c+1 is in flight
-                    // while chunk c is reduced to its parity bits
-                    const u32 tbase = tmem + ((u32)(ew * 32) << 16) + (u32)(acc * UN);
-                    u32 ra[32], rb[32];
-                    ptx::tmem_ld_32x32b_x32(tbase, ra);
-                    ptx::tmem_ld_wait();
-#pragma unroll
-                    for (int c = 0; c < UN / 32; c += 2) {
-                        ptx::tmem_ld_32x32b_x32(tbase + (u32)((c + 1) * 32), rb);
-                        u32 b = ra[0] & 1u;
-#pragma unroll
-                        for (int j = 1; j < 32; ++j) b = bfi1(ra[j], b, (u32)j);
-                        bits[c] = b;
-                        ptx::tmem_ld_wait();
-                        if (c + 2 < UN / 32) ptx::tmem_ld_32x32b_x32(tbase + (u32)((c + 2) * 32), ra);
-                        b = rb[0] & 1u;
-#pragma unroll
-                        for (int j = 1; j < 32; ++j) b = bfi1(rb[j], b, (u32)j);
-                        bits[c + 1] = b;
-                        if (c + 2 < UN / 32) ptx::tmem_ld_wait();
+                for (int c = 0; c < 2; ++c) {
+                    const int item = gt + 256 * c;
+                    const int slot = tile * UM + (item >> 2), q = item & 3;
+                    if (slot < nu) {
+                        row[c] = ulist[slot];
+                        if (q < nw) old[c] = M[(i64)row[c] * ld + w0 + q];
                     }
                 }
-                ptx::tc_fence_before();
-                ptx::mbar_arrive(&ctl->accempty[acc]);
-                if (dst) {
-                    u64 any = 0;
+                if (k > 0 && !drain_and_write()) ok = false;
+                ++k;
+                p_it = it;
+                p_w0 = w0;
+                p_nw = nw;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (q < nw) {
-                            const u64 v = old[q] ^ ((u64)bits[2 * q] | ((u64)bits[2 * q + 1] << 32));
-                            dst[q] = v;
-                            any |= v;
-                        }
-                    }
-                    if (any) live[urow] = 1;
+                for (int c = 0; c < 2; ++c) {
+                    p_row[c] = row[c];
+                    p_old[c] = old[c];
                 }
             }
         }
+        if (k > 0 && !drain_and_write()) ok = false;
         if (!ok) *abort_flag = 1;
     }
 
@@ -930,7 +970,7 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
         const i64 strips = (lw + 3) / 4;
         const i64 units_max = strips * ((L.mpad / UM + U_MCH - 1) / U_MCH);
         const int grid = (int)(units_max < sms ? units_max : sms);
-        tc_update_kernel<<<grid, 192, U_SMEM, s>>>(mx, mr, M, ld, wc, w, ws, ulist, live, err);
+        tc_update_kernel<<<grid, U_THREADS, U_SMEM, s>>>(mx, mr, M, ld, wc, w, ws, ulist, live, err);
     }
     MELA_LAUNCH_CHECK("tensor-core elimination");
     MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &ws->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));
