@@ -297,7 +297,7 @@ def bench_dense_rank(torch):
     out = {"config": "A = L*R mod 2, L 16384x12000, R 12000x32768 (seed 2), 164 rows replaced by XORs "
                      "of two others", "golden_rank": golden, "rank_ms": {}, "null_ms": {}}
     ranks = set()
-    for form in ("m4ri", "m4ri_k4", "plain"):
+    for form in ("tc", "m4ri", "m4ri_k4", "plain"):
         v = _lib.ELIM_VARIANTS[form]
         Mx = A.clone()
         torch.cuda.synchronize()
@@ -311,16 +311,37 @@ def bench_dense_rank(torch):
         ranks.add(int(dr.item()))
     r = ranks.pop() if len(ranks) == 1 else None
     out["rank"] = r
-    # null space through the blocked form: RREF + basis, then A * Z = 0 on the tensor cores
+    # work of forward elimination with these pivots: sum_t 2 (m - t - 1) (n - c_t) bit operations
+    piv = dpv[:r].cpu().numpy().astype(np.float64) if r else np.zeros(0)
+    t = np.arange(len(piv), dtype=np.float64)
+    ge_ops = float(np.sum(2.0 * (m - t - 1) * (n - piv)))
+    out["ge_bitops"] = ge_ops
+    out["rank_tbitops"] = {k: round(ge_ops / (v * 1e-3) / 1e12, 1) for k, v in out["rank_ms"].items()}
+    out["tc_over_m4ri_k4"] = round(out["rank_ms"]["m4ri_k4"] / out["rank_ms"]["tc"], 2)
+    out["tc_over_plain"] = round(out["rank_ms"]["plain"] / out["rank_ms"]["tc"], 2)
+    # RREF by the blocked form (for comparison), then by the tensor-core form + null basis,
+    # then A * Z = 0 on the tensor cores
     Mx = A.clone()
     torch.cuda.synchronize()
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
     e0.record()
     check(L.mela_dev_rref(_lib.ELIM_M4RI, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
                           dpr.data_ptr(), ws.data_ptr(), wsb, s))
     e1.record()
     e1.synchronize()
+    out["null_ms"]["m4ri_rref"] = round(e0.elapsed_time(e1), 2)
+    rows_m4ri = Mx[dpr[:int(dr.item())]].clone()
+    Mx = A.clone()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    check(L.mela_dev_rref(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                          dpr.data_ptr(), ws.data_ptr(), wsb, s))
+    e1.record()
+    e1.synchronize()
     rr = int(dr.item())
+    out["rref_rows_equal"] = bool(torch.equal(rows_m4ri, Mx[dpr[:rr]]))
+    del rows_m4ri
     f = n - rr
     Zt = torch.empty((f, wc), dtype=torch.int64, device="cuda")
     nwb = L.mela_null_workspace_size(n, rr)
@@ -330,7 +351,7 @@ def bench_dense_rank(torch):
                                 Zt.data_ptr(), wc, nws.data_ptr(), nwb, s))
     e2.record()
     e2.synchronize()
-    out["null_ms"]["m4ri_rref"] = round(e0.elapsed_time(e1), 2)
+    out["null_ms"]["tc_rref"] = round(e0.elapsed_time(e1), 2)
     out["null_ms"]["basis"] = round(e1.elapsed_time(e2), 2)
     Z = D.transpose(Zt, f, n)  # n x f
     prod = D.matmul(A, Z, m, n, f, variant="tc")

@@ -283,21 +283,21 @@ mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_p
  * time (microseconds) of each of a request's kernel variants from its
  * shape and density; the dispatcher takes the fastest prediction.  It only
  * chooses how a result is computed: every variant returns the same bits.
- * Parameters: one float array W1[8][32] b1[32] W2[32][32] b2[32] W3[32][4]
- * b3[4].  Variant order per output: products (plain, m4ri, tc, tc_fp4); rank and
- * null space (plain, m4ri, m4ri_k4, fused). */
+ * Parameters: one float array W1[8][32] b1[32] W2[32][32] b2[32] W3[32][5]
+ * b3[5].  Variant order per output: products (plain, m4ri, tc, tc_fp4; the
+ * fifth output unused); rank and null space (plain, m4ri, m4ri_k4, fused, tc). */
 #define MELA_MLP_IN 8
 #define MELA_MLP_H1 32
 #define MELA_MLP_H2 32
-#define MELA_MLP_OUT 4
-#define MELA_MLP_PARAMS 1476
+#define MELA_MLP_OUT 5
+#define MELA_MLP_PARAMS 1509
 typedef enum { MELA_OP_RANK = 0, MELA_OP_NULL = 1, MELA_OP_MATMUL = 2 } mela_op;
 
-/* Y (N x 4) = network(X (N x 8)) on the device. */
+/* Y (N x 5) = network(X (N x 8)) on the device. */
 mela_status mela_mlp_forward(const float *d_params, const float *d_X, int64_t N, float *d_Y,
                              void *stream);
 /* d_grad = gradient of the masked mean squared error between the network's
- * outputs and targets T (N x 4, mask 1 where observed), scaled by inv_count
+ * outputs and targets T (N x 5, mask 1 where observed), scaled by inv_count
  * = 1/(observed count); d_loss_sum (optional) = sum of squared errors. */
 mela_status mela_mlp_gradient(const float *d_params, const float *d_X, const float *d_T,
                               const float *d_mask, int64_t N, float inv_count, float *d_grad,
@@ -307,7 +307,7 @@ mela_status mela_mlp_adam_step(float *d_params, const float *d_grad, float *d_m1
                                int64_t step, float lr, void *stream);
 /* Install (or, with NULL, remove) the dispatch model from host memory. */
 mela_status mela_costmodel_load(const float *h_params);
-/* Variant index (0..3) the installed model picks, or -1 when none is
+/* Variant index (0..3 for products, 0..4 otherwise) the installed model picks, or -1 when none is
  * installed (the fixed rule is used then). */
 int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density);
 /* The 8 input features of a request. */

@@ -26,7 +26,7 @@ GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc"
 FN_MATMUL_GF2, FN_MATMUL_M4RI, FN_RANK_GF2, FN_RANK_M4RI, FN_NULL_GF2, FN_NULL_M4RI = range(6)
 # mela_op and the cost model's shape
 OP_RANK, OP_NULL, OP_MATMUL = 0, 1, 2
-MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 4, 1476
+MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 5, 1509
 # variant index (model output) -> variant code, per op
 OP_VARIANTS = {OP_MATMUL: (1, 2, 3, 4), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
 # mela_elim_variant

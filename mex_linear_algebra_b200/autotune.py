@@ -80,7 +80,7 @@ def time_elim(torch, op, m, n, density, stream_id, reps=3):
     piv = torch.empty(mn, dtype=torch.int64, device="cuda")
     prow = torch.empty(mn, dtype=torch.int64, device="cuda")
     times, results = {}, {}
-    for v, name in zip((_lib.ELIM_PLAIN, _lib.ELIM_M4RI, _lib.ELIM_M4RI_K4, _lib.ELIM_FUSED),
+    for v, name in zip((_lib.ELIM_PLAIN, _lib.ELIM_M4RI, _lib.ELIM_M4RI_K4, _lib.ELIM_FUSED, _lib.ELIM_TC),
                        VARIANT_NAMES[op]):
         ts = []
         for rep in range(reps + 1):

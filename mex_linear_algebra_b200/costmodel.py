@@ -23,8 +23,9 @@ from ._lib import check, lib
 PKG = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(PKG, "costmodel.json")
 OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL}
-VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc", "tc_fp4"), "rank": ("plain", "m4ri", "m4ri_k4", "fused"),
-                 "null": ("plain", "m4ri", "m4ri_k4", "fused")}
+VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc", "tc_fp4"),
+                 "rank": ("plain", "m4ri", "m4ri_k4", "fused", "tc"),
+                 "null": ("plain", "m4ri", "m4ri_k4", "fused", "tc")}
 
 
 def features(op: str, m: int, n: int, p: int, density: float) -> np.ndarray:
@@ -34,7 +35,7 @@ def features(op: str, m: int, n: int, p: int, density: float) -> np.ndarray:
 
 
 def dataset(records):
-    """Records (autotune DB rows) -> X (N x 8), T (N x 4 log2 us), mask (N x 4)."""
+    """Records (autotune DB rows) -> X (N x 8), T (N x 5 log2 us), mask (N x 5)."""
     X = np.stack([features(r["op"], r["m"], r["n"], r.get("p", 0), r["density"]) for r in records])
     T = np.zeros((len(records), _lib.MLP_OUT), dtype=np.float32)
     Mk = np.zeros_like(T)
@@ -128,7 +129,7 @@ def heuristic(op: str, m: int, n: int, p: int, density: float) -> str:
     """The library's fixed rule (what dispatch does without a model)."""
     if op == "matmul":
         return "tc" if (m >= 1024 and n >= 1024 and p >= 1024) else "plain"
-    return "m4ri"
+    return "fused" if m * n < 65536 else "tc"
 
 
 def evaluate(params: np.ndarray, records):

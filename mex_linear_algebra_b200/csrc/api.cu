@@ -79,6 +79,8 @@ int sm_count()
 // calls, so repeated gateway calls do not pay cudaMalloc).
 struct HostCtx {
     cudaStream_t stream[kMaxDevices] = {};
+    cudaStream_t copy_in[kMaxDevices] = {};   // pipelined host products: uploads
+    cudaStream_t copy_out[kMaxDevices] = {};  //   and downloads
 };
 static thread_local HostCtx t_ctx;
 
@@ -100,6 +102,17 @@ mela_status host_stream(cudaStream_t *s)
         }
     }
     *s = t_ctx.stream[d];
+    return MELA_OK;
+}
+
+// The calling thread's upload and download streams (created on first use).
+static mela_status copy_streams(cudaStream_t *in, cudaStream_t *out)
+{
+    const int d = current_device();
+    if (!t_ctx.copy_in[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.copy_in[d], cudaStreamNonBlocking));
+    if (!t_ctx.copy_out[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.copy_out[d], cudaStreamNonBlocking));
+    *in = t_ctx.copy_in[d];
+    *out = t_ctx.copy_out[d];
     return MELA_OK;
 }
 
@@ -416,6 +429,103 @@ extern "C" mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, 
                     workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
+// Tensor-core product of host matrices with the transfers overlapped: B is
+// uploaded and prepared first; A goes up in blocks of rows on the
+// upload stream, each block is expanded and multiplied on the compute stream
+// as soon as it has arrived, and its rows of C go down on the download stream
+// while the next block is multiplied.  (With page-locked host buffers the
+// three streams run concurrently; pageable buffers still give the right
+// result, with less overlap.)
+static constexpr i64 kPipeRows = 4096;
+
+static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, const uint64_t *B, int64_t ldb,
+                                                uint64_t *C, int64_t ldc, i64 m, i64 k, i64 n, int variant,
+                                                cudaStream_t s)
+{
+    cudaStream_t sin, sout;
+    mela_status st = copy_streams(&sin, &sout);
+    if (st != MELA_OK) return st;
+    const bool fp4 = variant == MELA_GEMM_TC_FP4;
+    if (fp4 && k >= (1LL << 24)) {
+        set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+        return MELA_ERR_UNSUPPORTED;
+    }
+    const GemmPlan p = plan_gemm(variant, m, k, n);
+    const i64 wk = words_of(k), wn = words_of(n);
+    // blocks of kPipeRows rows, larger (a multiple of 128) when that would make more than 64
+    i64 brows = (m + 63) / 64;
+    brows = brows < kPipeRows ? kPipeRows : (brows + 127) / 128 * 128;
+    const i64 nblk = (m + brows - 1) / brows;
+    DevBuf dA, dB, dC, ws;
+    if ((st = dA.alloc((size_t)m * wk * 8, s)) != MELA_OK) return st;
+    if ((st = dB.alloc((size_t)k * wn * 8, s)) != MELA_OK) return st;
+    if ((st = dC.alloc((size_t)m * wn * 8, s)) != MELA_OK) return st;
+    if ((st = ws.alloc(p.total, s)) != MELA_OK) return st;
+    const GemmBufs b = carve(p, ws.p);
+    u64 *a = (u64 *)dA.p, *bb = (u64 *)dB.p, *c = (u64 *)dC.p;
+
+    // events: buffers allocated (s), block i uploaded (sin), block i multiplied (s)
+    const int nev = 1 + 2 * (int)nblk + 2;
+    cudaEvent_t evs[1 + 2 * 64 + 2];
+    int made = 0;
+    auto cleanup = [&]() {
+        for (int i = 0; i < made; ++i) cudaEventDestroy(evs[i]);
+    };
+    for (; made < nev; ++made) {
+        if (cudaEventCreateWithFlags(&evs[made], cudaEventDisableTiming) != cudaSuccess) {
+            cleanup();
+            set_error("cudaEventCreate failed");
+            return MELA_ERR_CUDA;
+        }
+    }
+    cudaEvent_t ev_alloc = evs[0], ev_done_in = evs[nev - 2], ev_done_out = evs[nev - 1];
+    auto ev_up = [&](i64 i) { return evs[1 + i]; };
+    auto ev_mul = [&](i64 i) { return evs[1 + nblk + i]; };
+    auto run = [&]() -> mela_status {
+        MELA_CUDA_TRY(cudaEventRecord(ev_alloc, s));
+        MELA_CUDA_TRY(cudaStreamWaitEvent(sin, ev_alloc, 0));
+        MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_alloc, 0));
+        // B first: the whole of it is needed by every block
+        MELA_CUDA_TRY(cudaMemcpy2DAsync(bb, (size_t)wn * 8, B, (size_t)ldb * 8, (size_t)wn * 8, (size_t)k,
+                                        cudaMemcpyHostToDevice, s));
+        for (i64 i = 0; i < nblk; ++i) {
+            const i64 r0 = i * brows, rows = (m - r0) < brows ? (m - r0) : brows;
+            MELA_CUDA_TRY(cudaMemcpy2DAsync(a + r0 * wk, (size_t)wk * 8, A + r0 * lda, (size_t)lda * 8,
+                                            (size_t)wk * 8, (size_t)rows, cudaMemcpyHostToDevice, sin));
+            MELA_CUDA_TRY(cudaEventRecord(ev_up(i), sin));
+        }
+        mela_status st2 = launch_transpose(bb, wn, k, n, b.Bt, p.ldbt, s);
+        if (st2 != MELA_OK) return st2;
+        if (p.ldbt > wk) MELA_CUDA_TRY(cudaMemset2DAsync(b.Bt + wk, (size_t)p.ldbt * 8, 0, 8, (size_t)n, s));
+        st2 = fp4 ? launch_expand_f4(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)
+                  : launch_expand_u8(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s);
+        if (st2 != MELA_OK) return st2;
+        for (i64 i = 0; i < nblk; ++i) {
+            const i64 r0 = i * brows, rows = (m - r0) < brows ? (m - r0) : brows;
+            const i64 rp = (rows + 127) / 128 * 128;
+            unsigned char *a8 = b.A8 + (size_t)r0 * p.kp;
+            MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_up(i), 0));
+            st2 = fp4 ? launch_expand_f4(a + r0 * wk, wk, rows, k, rp, p.kp, a8, s)
+                      : launch_expand_u8(a + r0 * wk, wk, rows, k, rp, p.kp, a8, s);
+            if (st2 != MELA_OK) return st2;
+            st2 = launch_gemm_tc(a8, b.B8, rp, p.np, p.kp, c + r0 * wn, wn, rows, n, s, fp4);
+            if (st2 != MELA_OK) return st2;
+            MELA_CUDA_TRY(cudaEventRecord(ev_mul(i), s));
+            MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_mul(i), 0));
+            MELA_CUDA_TRY(cudaMemcpy2DAsync(C + r0 * ldc, (size_t)ldc * 8, c + r0 * wn, (size_t)wn * 8,
+                                            (size_t)wn * 8, (size_t)rows, cudaMemcpyDeviceToHost, sout));
+        }
+        return MELA_OK;
+    };
+    st = run();
+    // the buffers are released on s: it waits for both copy streams first
+    if (cudaEventRecord(ev_done_in, sin) == cudaSuccess) cudaStreamWaitEvent(s, ev_done_in, 0);
+    if (cudaEventRecord(ev_done_out, sout) == cudaSuccess) cudaStreamWaitEvent(s, ev_done_out, 0);
+    const mela_status fin = finish(s);
+    cleanup();
+    return st != MELA_OK ? st : fin;
+}
+
 extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, const uint64_t *B,
                                                int64_t ldb, uint64_t *C, int64_t ldc, int64_t m,
                                                int64_t k, int64_t n, int32_t variant)
@@ -429,6 +539,11 @@ extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, c
     cudaStream_t s;
     mela_status st = host_stream(&s);
     if (st != MELA_OK) return st;
+    {
+        const int v = plan_gemm(variant, m, k, n).variant;
+        if ((v == MELA_GEMM_TC || v == MELA_GEMM_TC_FP4) && k > 0 && m >= 2 * kPipeRows)
+            return matmul_packed_host_pipelined(A, lda, B, ldb, C, ldc, m, k, n, v, s);
+    }
     const i64 wk = words_of(k), wn = words_of(n);
     DevBuf dA, dB, dC, ws;
     if ((st = dA.alloc((size_t)m * (wk ? wk : 1) * 8, s)) != MELA_OK) return st;

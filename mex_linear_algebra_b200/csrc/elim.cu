@@ -547,9 +547,10 @@ size_t elim_workspace(i64 m, i64 n)
 int choose_elim_variant(i64 m, i64 n, int rref)
 {
     const int c = costmodel_choose(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0, 0.5);
-    static const int order[4] = {MELA_ELIM_PLAIN, MELA_ELIM_M4RI, MELA_ELIM_M4RI_K4, MELA_ELIM_FUSED};
-    if (c >= 0 && c < 4) return order[c];
-    return MELA_ELIM_M4RI;  // fixed rule: the blocked form
+    static const int order[5] = {MELA_ELIM_PLAIN, MELA_ELIM_M4RI, MELA_ELIM_M4RI_K4, MELA_ELIM_FUSED, MELA_ELIM_TC};
+    if (c >= 0 && c < 5) return order[c];
+    // fixed rule: one CTA for small matrices, tensor-core windows otherwise
+    return (double)m * (double)n < 65536.0 ? MELA_ELIM_FUSED : MELA_ELIM_TC;
 }
 
 mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank,

@@ -2,10 +2,10 @@
 // hand-written kernels, used to choose how (never what) each request is
 // computed.
 //
-// Network: x (8 features) -> 32 ReLU -> 32 ReLU -> 4 outputs, the predicted
-// log2 running time (microseconds) of each of the request's four kernel
-// variants.  Parameters are one flat float array:
-//   W1[8][32] b1[32] W2[32][32] b2[32] W3[32][4] b3[4]   (1476 floats)
+// Network: x (8 features) -> 32 ReLU -> 32 ReLU -> 5 outputs, the predicted
+// log2 running time (microseconds) of each of the request's kernel variants
+// (four products, five eliminations).  Parameters are one flat float array:
+//   W1[8][32] b1[32] W2[32][32] b2[32] W3[32][5] b3[5]   (1509 floats)
 // Loss: mean squared error over the observed (sample, variant) pairs.
 //
 // Kernels: forward (one thread per sample), backward (one thread per sample,
@@ -205,7 +205,8 @@ int costmodel_choose(int op, double m, double n, double p, double density)
     float x[kIn], y[kOut];
     costmodel_features(op, m, n, p, density, x);
     host_forward(P, x, y);
-    const int nv = 4;  // products: plain, m4ri, tc, tc_fp4; elimination: plain, m4ri, m4ri_k4, fused
+    // products: plain, m4ri, tc, tc_fp4; elimination: plain, m4ri, m4ri_k4, fused, tc
+    const int nv = op == MELA_OP_MATMUL ? 4 : 5;
     int best = 0;
     for (int o = 1; o < nv; ++o)
         if (y[o] < y[best]) best = o;

@@ -183,3 +183,28 @@ def test_fp4_variants_agree_large(cuda):
     A = D.rand_dense(13, 0, m, k)
     B = D.rand_dense(13, 1, k, n)
     assert torch.equal(D.matmul(A, B, m, k, n, variant="tc_fp4"), D.matmul(A, B, m, k, n, variant="tc"))
+
+
+@pytest.mark.parametrize("variant", ["tc", "tc_fp4", "plain"])
+@pytest.mark.parametrize("shape", [(9000, 1000, 700), (8192, 64, 65), (20000, 300, 256)])
+def test_packed_host_product(cuda, variant, shape):
+    """The host-buffer product (transfers overlapped in row blocks for the
+    tensor-core forms once m >= 8192) equals the device product of the oracle's
+    inputs, including a ragged last block and page-locked and pageable buffers."""
+    import torch
+    from mex_linear_algebra_b200 import _lib
+    m, k, n = shape
+    A = O.rand_dense(61, m + k, m, k)
+    B = O.rand_dense(61, k + n, k, n)
+    wk, wn = (k + 63) // 64, (n + 63) // 64
+    want = to_host(_dev().matmul(to_dev(A), to_dev(B), m, k, n, variant="plain"))
+    for pinned in (True, False):
+        hA = torch.from_numpy(np.ascontiguousarray(A[:, :wk]).view(np.int64))
+        hB = torch.from_numpy(np.ascontiguousarray(B[:, :wn]).view(np.int64))
+        hC = torch.zeros((m, wn), dtype=torch.int64)
+        if pinned:
+            hA, hB, hC = hA.pin_memory(), hB.pin_memory(), hC.pin_memory()
+        _lib.check(_lib.lib().mela_matmul_packed_host(hA.data_ptr(), wk, hB.data_ptr(), wn, hC.data_ptr(), wn,
+                                                      m, k, n, _lib.GEMM_VARIANTS[variant]))
+        got = hC.numpy().view(np.uint64)
+        assert np.array_equal(valid_words(got, n), valid_words(want, n)), (variant, pinned)
