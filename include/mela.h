@@ -71,7 +71,7 @@ typedef enum {
     MELA_GEMM_M4RI = 2,   /* Four-Russians tables in shared memory */
     MELA_GEMM_TC = 3,     /* tcgen05 kind::i8 tensor cores, parity of the s32 sum */
     MELA_GEMM_TC_FP4 = 4  /* tcgen05 kind::mxf4 (e2m1 0/1, unit scales), parity of the exact
-                             f32 sum; k < 2^24 */
+                             f32 sum; k < 2^23 */
 } mela_gemm_variant;
 
 /* Elimination variants (rank / RREF / null space); results are identical. */

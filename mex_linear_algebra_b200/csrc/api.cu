@@ -170,7 +170,7 @@ int choose_gemm_variant(i64 m, i64 k, i64 n)
     if (c >= 0) {
         static const int order[4] = {MELA_GEMM_PLAIN, MELA_GEMM_M4RI, MELA_GEMM_TC, MELA_GEMM_TC_FP4};
         const int v = order[c & 3];
-        if (v == MELA_GEMM_TC_FP4 && k >= (1LL << 24)) return MELA_GEMM_TC;
+        if (v == MELA_GEMM_TC_FP4 && k >= (1LL << 23)) return MELA_GEMM_TC;
         return v;
     }
     // fixed rule: tensor cores pay off once every dimension spans a few
@@ -188,14 +188,14 @@ static GemmPlan plan_gemm(int variant, i64 m, i64 k, i64 n)
     if (variant == MELA_GEMM_PLAIN || variant == MELA_GEMM_TC || variant == MELA_GEMM_TC_FP4)
         p.bt_bytes = (size_t)n * p.ldbt * 8;
     if (variant == MELA_GEMM_TC) {
-        p.mp = round_up(m, 128);
+        p.mp = round_up(m, 256);  // 256-row tiles for CTA pairs
         p.np = round_up(n, 256);
         p.kp = round_up(k, 128);  // bytes = values
         p.a8_bytes = (size_t)p.mp * p.kp;
         p.b8_bytes = (size_t)p.np * p.kp;
     }
     if (variant == MELA_GEMM_TC_FP4) {
-        p.mp = round_up(m, 128);
+        p.mp = round_up(m, 256);
         p.np = round_up(n, 256);
         p.kp = round_up(k, 256) / 2;  // bytes, two values each
         p.a8_bytes = (size_t)p.mp * p.kp;
@@ -241,8 +241,8 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
     mela_status st = check_ws(p, ws, ws_bytes);
     if (st != MELA_OK) return st;
     GemmBufs b = carve(p, ws);
-    if (p.variant == MELA_GEMM_TC_FP4 && k >= (1LL << 24)) {
-        set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+    if (p.variant == MELA_GEMM_TC_FP4 && k >= (1LL << 23)) {
+        set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
         return MELA_ERR_UNSUPPORTED;
     }
     if (p.variant == MELA_GEMM_PLAIN || p.variant == MELA_GEMM_TC || p.variant == MELA_GEMM_TC_FP4) {
@@ -280,8 +280,8 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
     case MELA_GEMM_PLAIN: return launch_gemm_plain(A, lda, b.Bt, p.ldbt, C, ldc, m, k, n, s);
     case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, false);
     case MELA_GEMM_TC_FP4:
-        if (k >= (1LL << 24)) {
-            set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+        if (k >= (1LL << 23)) {
+            set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
             return MELA_ERR_UNSUPPORTED;
         }
         return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, true);
@@ -446,15 +446,15 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
     mela_status st = copy_streams(&sin, &sout);
     if (st != MELA_OK) return st;
     const bool fp4 = variant == MELA_GEMM_TC_FP4;
-    if (fp4 && k >= (1LL << 24)) {
-        set_error("fp4 tensor-core product needs k < 2^24 (exact f32 sums)");
+    if (fp4 && k >= (1LL << 23)) {
+        set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
         return MELA_ERR_UNSUPPORTED;
     }
     const GemmPlan p = plan_gemm(variant, m, k, n);
     const i64 wk = words_of(k), wn = words_of(n);
-    // blocks of kPipeRows rows, larger (a multiple of 128) when that would make more than 64
+    // blocks of kPipeRows rows, larger (a multiple of 256) when that would make more than 64
     i64 brows = (m + 63) / 64;
-    brows = brows < kPipeRows ? kPipeRows : (brows + 127) / 128 * 128;
+    brows = brows < kPipeRows ? kPipeRows : (brows + 255) / 256 * 256;
     const i64 nblk = (m + brows - 1) / brows;
     DevBuf dA, dB, dC, ws;
     if ((st = dA.alloc((size_t)m * wk * 8, s)) != MELA_OK) return st;
@@ -502,7 +502,7 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
         if (st2 != MELA_OK) return st2;
         for (i64 i = 0; i < nblk; ++i) {
             const i64 r0 = i * brows, rows = (m - r0) < brows ? (m - r0) : brows;
-            const i64 rp = (rows + 127) / 128 * 128;
+            const i64 rp = (rows + 255) / 256 * 256;
             unsigned char *a8 = b.A8 + (size_t)r0 * p.kp;
             MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_up(i), 0));
             st2 = fp4 ? launch_expand_f4(a + r0 * wk, wk, rows, k, rp, p.kp, a8, s)

@@ -23,8 +23,12 @@
 // UE8M0 scale factor per 32 values of K, at twice the INT8 rate.  Every scale
 // factor is 1.0, so the scale-factor columns of TMEM are one constant block
 // (bytes 0x7F) written once per CTA and addressed by every instruction.  The
-// f32 accumulator holds the integer dot product exactly while it is below
-// 2^24, so K < 2^24 is required; the parity bit is that of the integer.
+// f32 accumulator holds the integer dot product exactly; K < 2^23 is
+// required so that adding 2^23 puts the integer in the low mantissa bits,
+// whose bit 0 is the parity (one float add per value instead of a
+// float-to-int conversion).
+#include <cstdlib>
+
 #include "mela_common.cuh"
 #include "mela_internal.h"
 #include "tc_ptx.cuh"
@@ -187,7 +191,7 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 u32 b = 0;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const u32 v = F4 ? (u32)__float2int_rz(__uint_as_float(r[j])) : r[j];
+                    const u32 v = F4 ? __float_as_uint(__uint_as_float(r[j]) + 8388608.0f) : r[j];
                     b |= (v & 1u) << j;
                 }
                 bits[c] = b;
@@ -208,6 +212,187 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (warp == 1) {
         ptx::tc_fence_after();
         ptx::tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------- CTA pairs
+// The same product with 256 x 256 output tiles computed by a cluster of two
+// CTAs (tcgen05 cta_group::2).  CTA r of the pair loads rows r*128..+127 of
+// the tile's A rows and of its B rows (B transposed) into its own shared
+// memory; the TMA completions of both CTAs are counted on the even CTA's
+// stage barrier, and the even CTA's MMA thread issues M = 256 instructions
+// that read both CTAs' halves and accumulate, in each CTA's TMEM, that CTA's
+// 128 rows x 256 columns.  Each SM thereby fills half as many B bytes into
+// shared memory per instruction as with one CTA per tile.  The MMA commits
+// arrive on the barrier of the same offset in both CTAs, so each CTA's
+// producer learns when a stage is free and each CTA's epilogue when its
+// accumulator is ready.  No TMA load uses cluster multicast.
+namespace {
+constexpr int P_STAGES = 7;
+constexpr int P_A_BYTES = 128 * BK;                    // this CTA's 128 rows of A
+constexpr int P_B_BYTES = 128 * BK;                    // this CTA's 128 rows of B
+constexpr int P_STAGE_BYTES = P_A_BYTES + P_B_BYTES;
+constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
+
+struct PairCtl {
+    u64 full[P_STAGES];   // even CTA: both CTAs' bytes of a stage have landed
+    u64 empty[P_STAGES];  // both CTAs: the pair's MMAs have read a stage
+    u64 acc;              // both CTAs: the accumulator is complete
+    u64 drain;
+    u32 tmem;
+    int abort;
+};
+}  // namespace
+
+template <bool F4>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    u64 *__restrict__ C, i64 ldc, i64 m, i64 n, int tiles_m, int tiles_n, int kstages, u32 *err)
+{
+    constexpr u32 TMEM_COLS = F4 ? 512 : 256;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    PairCtl *ctl = reinterpret_cast<PairCtl *>(smem + P_STAGES * P_STAGE_BYTES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 rank = ptx::cluster_ctarank();
+    const bool leader = rank == 0;
+
+    // grouped rasterisation over 256 x 256 tiles
+    const int t = blockIdx.x >> 1;
+    const int per_group = GROUP_M * tiles_n;
+    const int group = t / per_group;
+    const int first_m = group * GROUP_M;
+    const int gsize = (tiles_m - first_m) < GROUP_M ? (tiles_m - first_m) : GROUP_M;
+    const int tm = first_m + (t % per_group) % gsize;
+    const int tn = (t % per_group) / gsize;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P_STAGES; ++s) {
+            ptx::mbar_init(&ctl->full[s], 1);
+            ptx::mbar_init(&ctl->empty[s], 1);
+        }
+        ptx::mbar_init(&ctl->acc, 1);
+        ptx::mbar_init(&ctl->drain, 1);
+        ctl->abort = 0;
+        ptx::fence_barrier_init();
+    }
+    if (warp == 0 && lane == 0) {
+        ptx::prefetch_tmap(&tmA);
+        ptx::prefetch_tmap(&tmB);
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc_pair(&ctl->tmem, TMEM_COLS);
+        ptx::tmem_relinquish_pair();
+    }
+    ptx::tc_fence_before();
+    ptx::cluster_sync();  // both CTAs' barriers and TMEM exist before any copy or MMA
+    ptx::tc_fence_after();
+    const u32 tmem = ctl->tmem;
+    volatile int *abort_flag = &ctl->abort;
+    if constexpr (F4) {
+        if (warp >= 2) {
+            const u32 lane_base = (u32)((warp & 3) * 32) << 16;
+            ptx::tmem_st_32x32b_x16(tmem + lane_base + SF_COL, 0x7F7F7F7Fu);
+            ptx::tmem_st_32x32b_x16(tmem + lane_base + SF_COL + 16, 0x7F7F7F7Fu);
+            ptx::tmem_st_wait();
+        }
+        ptx::tc_fence_before();
+        ptx::cluster_sync();  // the scale factors of both CTAs are in place
+        ptx::tc_fence_after();
+    }
+
+    if (warp == 0) {
+        if (lane == 0) {
+            const u32 full0 = ptx::mapa_shared(ptx::smem_u32(&ctl->full[0]), 0);
+            for (int ks = 0; ks < kstages; ++ks) {
+                const int s = ks % P_STAGES, round = ks / P_STAGES;
+                if (round > 0 && !ptx::mbar_wait(&ctl->empty[s], (round - 1) & 1, err)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                unsigned char *sa = smem + s * P_STAGE_BYTES;
+                if (leader) ptx::mbar_arrive_expect_tx(&ctl->full[s], 2 * P_STAGE_BYTES);
+                const u32 bar = full0 + (u32)(s * sizeof(u64));
+                ptx::tma_load_2d_pair(sa, &tmA, bar, ks * BK, tm * 256 + (int)rank * 128);
+                ptx::tma_load_2d_pair(sa + P_A_BYTES, &tmB, bar, ks * BK, tn * 256 + (int)rank * 128);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            constexpr u32 idesc = F4 ? ptx::idesc_mxf4(256, BN) : ptx::idesc_i8(256, BN);
+            bool ok = true;
+            for (int ks = 0; ks < kstages; ++ks) {
+                const int s = ks % P_STAGES, round = ks / P_STAGES;
+                if (!ptx::mbar_wait(&ctl->full[s], round & 1, err) || *abort_flag) {
+                    *abort_flag = 1;
+                    ok = false;
+                    break;
+                }
+                ptx::tc_fence_after();
+                const u32 a0 = ptx::smem_u32(smem + s * P_STAGE_BYTES);
+                const u32 b0 = a0 + P_A_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < BK / 32; ++kk) {
+                    if constexpr (F4)
+                        ptx::umma_mxf4_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
+                                            idesc, tmem + SF_COL, tmem + SF_COL + 8, (ks | kk) != 0);
+                    else
+                        ptx::umma_i8_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
+                                          idesc, (ks | kk) != 0);
+                }
+                ptx::umma_commit_pair(&ctl->empty[s], 0x3);
+            }
+            if (ok) {
+                ptx::umma_commit_pair(&ctl->acc, 0x3);
+            } else {
+                // drain the MMAs still reading either CTA's shared memory
+                ptx::umma_commit_pair(&ctl->drain, 0x1);
+                ptx::mbar_wait(&ctl->drain, 0, nullptr);
+            }
+        }
+        __syncwarp();
+    } else {
+        const bool ok = ptx::mbar_wait(&ctl->acc, 0, err);
+        ptx::tc_fence_after();
+        if (ok && !*abort_flag) {
+            const int ew = warp & 3;  // TMEM lane quarter this warp may access
+            const i64 row = (i64)tm * 256 + (i64)rank * 128 + ew * 32 + lane;
+            u32 bits[BN / 32];
+#pragma unroll
+            for (int c = 0; c < BN / 32; ++c) {
+                u32 r[32];
+                ptx::tmem_ld_32x32b_x32(tmem + ((u32)(ew * 32) << 16) + (u32)(c * 32), r);
+                ptx::tmem_ld_wait();
+                u32 b = 0;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const u32 v = F4 ? __float_as_uint(__uint_as_float(r[j]) + 8388608.0f) : r[j];
+                    b |= (v & 1u) << j;
+                }
+                bits[c] = b;
+            }
+            const i64 nw = words_of(n);
+            if (row < m) {
+#pragma unroll
+                for (int q = 0; q < BN / 64; ++q) {
+                    const i64 w = (i64)tn * (BN / 64) + q;
+                    if (w < nw) C[row * ldc + w] = (u64)bits[2 * q] | ((u64)bits[2 * q + 1] << 32);
+                }
+            }
+        } else {
+            *abort_flag = 1;
+        }
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::cluster_sync();  // neither CTA leaves while the pair's MMAs may still read its shared memory
+    if (warp == 1) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc_pair(tmem, TMEM_COLS);
     }
 }
 
@@ -259,6 +444,15 @@ mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 
     return make_map(map, base, rows, kp, box_rows);
 }
 
+// CTA pairs are used whenever the padded row count allows (mp % 256 == 0),
+// unless MELA_TC_PAIR=0 is set in the environment (one CTA per 128 x 256 tile).
+static bool use_pairs(i64 mp)
+{
+    if (mp % 256) return false;
+    const char *e = getenv("MELA_TC_PAIR");
+    return !(e && e[0] == '0');
+}
+
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
                            i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4)
 {
@@ -275,6 +469,27 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
     if (tiles_m * tiles_n > 0x7fffffffLL || kst > 0x7fffffffLL || kp > (1LL << 31)) {
         set_error("gemm_tc: problem too large for one launch");
         return MELA_ERR_UNSUPPORTED;
+    }
+    if (use_pairs(mp)) {
+        CUtensorMap ma, mb;
+        mela_status st = make_map(&ma, A8, mp, kp, 128);
+        if (st != MELA_OK) return st;
+        st = make_map(&mb, Bt8, np, kp, 128);
+        if (st != MELA_OK) return st;
+        const unsigned grid = (unsigned)(2 * (mp / 256) * tiles_n);
+        if (fp4) {
+            MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_pair_kernel<true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            gemm_tc_pair_kernel<true><<<grid, 192, P_SMEM_BYTES, s>>>(ma, mb, C, ldc, m, n, (int)(mp / 256),
+                                                                       (int)tiles_n, (int)kst, device_error_word());
+        } else {
+            MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_pair_kernel<false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            gemm_tc_pair_kernel<false><<<grid, 192, P_SMEM_BYTES, s>>>(ma, mb, C, ldc, m, n, (int)(mp / 256),
+                                                                        (int)tiles_n, (int)kst, device_error_word());
+        }
+        MELA_LAUNCH_CHECK("gemm_tc_pair_kernel");
+        return MELA_OK;
     }
     CUtensorMap ma, mb;
     mela_status st = make_map(&ma, A8, mp, kp, BM);
