@@ -550,8 +550,12 @@ def run_mela(args, ws, rank, local):
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "result_check": "ok" if ok else "MISMATCH"},
             "roofline": {"bound": "tensor", "achieved": round(achieved, 1), "peak": round(peak, 1),
-                         "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": None,
-                         "kernel": "gemm_tc_kernel", "kernel_ms": round(kern_avg, 4),
+                         "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                         # dram read + write bytes of one launch: ncu capture at 16384^3 (FP4, 0.715 GB)
+                         # scaled by m*n*k to the full launch (profiles/gemm_tc_pair_kernel_fp4_32768.md)
+                         "traffic": (0.7154e9 * (M * N * K) / 16384 ** 3) if args.variant == "tc_fp4" else None,
+                         "traffic_unit": "bytes per launch",
+                         "kernel": "gemm_tc_pair_kernel", "kernel_ms": round(kern_avg, 4),
                          "peak_source": ("2 x dense INT8 measured in this run (cuBLASLt int8 GEMM 8192^3 "
                                          "via torch._int_mm, best of 10): the FP4 rate is twice the INT8 "
                                          "rate" if args.variant == "tc_fp4" else
