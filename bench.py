@@ -551,8 +551,8 @@ def run_mela(args, ws, rank, local):
                        "result_check": "ok" if ok else "MISMATCH"},
             "roofline": {"bound": "tensor", "achieved": round(achieved, 1), "peak": round(peak, 1),
                          "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
-                         # dram read + write bytes of one launch: ncu capture at 16384^3 (FP4, 0.715 GB)
-                         # scaled by m*n*k to the full launch (profiles/gemm_tc_pair_kernel_fp4_32768.md)
+                         # dram read + write bytes of one launch: an ncu capture of the FP4 kernel at
+                         # 16384^3 (0.715 GB) scaled by m*n*k to the full launch
                          "traffic": (0.7154e9 * (M * N * K) / 16384 ** 3) if args.variant == "tc_fp4" else None,
                          "traffic_unit": "bytes per launch",
                          "kernel": "gemm_tc_pair_kernel", "kernel_ms": round(kern_avg, 4),
