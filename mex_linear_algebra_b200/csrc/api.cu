@@ -429,14 +429,17 @@ extern "C" mela_status mela_dev_matmul_run(int32_t variant, const uint64_t *dA, 
                     workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
-// Tensor-core product of host matrices with the transfers overlapped: B is
-// uploaded and prepared first; A goes up in blocks of rows on the
-// upload stream, each block is expanded and multiplied on the compute stream
-// as soon as it has arrived, and its rows of C go down on the download stream
-// while the next block is multiplied.  (With page-locked host buffers the
-// three streams run concurrently; pageable buffers still give the right
-// result, with less overlap.)
-static constexpr i64 kPipeRows = 4096;
+// Tensor-core product of host matrices with the transfers overlapped.  A is
+// cut into row blocks A_i and B into column blocks B_j (up to 4 x 4); the
+// upload stream sends A_0, B_0, A_1, B_1, ...; the compute stream prepares
+// each block as it lands (A_i expanded; B_j transposed and expanded) and runs
+// the product C_ij = A_i B_j as soon as both of its blocks are in, in the
+// order (i, j <= i) after A_i and (i <= j, j) after B_j; the download stream
+// sends each C_ij back while the next one is computed.  The first product thus
+// starts after two blocks have landed rather than after all of B.  (With
+// page-locked host buffers the three streams run concurrently; pageable
+// buffers still give the right result, with less overlap.)
+static constexpr i64 kPipeMin = 8192;  // pipelined when m and n both reach this
 
 static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, const uint64_t *B, int64_t ldb,
                                                 uint64_t *C, int64_t ldc, i64 m, i64 k, i64 n, int variant,
@@ -452,10 +455,9 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
     }
     const GemmPlan p = plan_gemm(variant, m, k, n);
     const i64 wk = words_of(k), wn = words_of(n);
-    // blocks of kPipeRows rows, larger (a multiple of 256) when that would make more than 64
-    i64 brows = (m + 63) / 64;
-    brows = brows < kPipeRows ? kPipeRows : (brows + 255) / 256 * 256;
-    const i64 nblk = (m + brows - 1) / brows;
+    // blocks: a multiple of 256 rows (columns), at most 4 per operand
+    const i64 mb = round_up((m + 3) / 4, 256), nb = round_up((n + 3) / 4, 256);
+    const int bm = (int)((m + mb - 1) / mb), bn = (int)((n + nb - 1) / nb);
     DevBuf dA, dB, dC, ws;
     if ((st = dA.alloc((size_t)m * wk * 8, s)) != MELA_OK) return st;
     if ((st = dB.alloc((size_t)k * wn * 8, s)) != MELA_OK) return st;
@@ -464,9 +466,10 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
     const GemmBufs b = carve(p, ws.p);
     u64 *a = (u64 *)dA.p, *bb = (u64 *)dB.p, *c = (u64 *)dC.p;
 
-    // events: buffers allocated (s), block i uploaded (sin), block i multiplied (s)
-    const int nev = 1 + 2 * (int)nblk + 2;
-    cudaEvent_t evs[1 + 2 * 64 + 2];
+    // events: buffers allocated; A_i uploaded; B_j uploaded; C_ij computed; copy streams done
+    constexpr int kMaxEv = 1 + 4 + 4 + 16 + 2;
+    cudaEvent_t evs[kMaxEv];
+    const int nev = 1 + bm + bn + bm * bn + 2;
     int made = 0;
     auto cleanup = [&]() {
         for (int i = 0; i < made; ++i) cudaEventDestroy(evs[i]);
@@ -479,41 +482,71 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
         }
     }
     cudaEvent_t ev_alloc = evs[0], ev_done_in = evs[nev - 2], ev_done_out = evs[nev - 1];
-    auto ev_up = [&](i64 i) { return evs[1 + i]; };
-    auto ev_mul = [&](i64 i) { return evs[1 + nblk + i]; };
+    auto ev_a = [&](int i) { return evs[1 + i]; };
+    auto ev_b = [&](int j) { return evs[1 + bm + j]; };
+    auto ev_c = [&](int i, int j) { return evs[1 + bm + bn + i * bn + j]; };
+    auto rows_of = [&](int i) { return (m - i * mb) < mb ? (m - i * mb) : mb; };
+    auto cols_of = [&](int j) { return (n - j * nb) < nb ? (n - j * nb) : nb; };
+
+    auto product = [&](int i, int j) -> mela_status {
+        const i64 r0 = i * mb, c0 = j * nb, rows = rows_of(i), cols = cols_of(j);
+        mela_status e = launch_gemm_tc(b.A8 + (size_t)r0 * p.kp, b.B8 + (size_t)c0 * p.kp, round_up(rows, 256),
+                                       round_up(cols, 256), p.kp, c + r0 * wn + c0 / 64, wn, rows, cols, s, fp4);
+        if (e != MELA_OK) return e;
+        MELA_CUDA_TRY(cudaEventRecord(ev_c(i, j), s));
+        MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_c(i, j), 0));
+        MELA_CUDA_TRY(cudaMemcpy2DAsync(C + r0 * ldc + c0 / 64, (size_t)ldc * 8, c + r0 * wn + c0 / 64,
+                                        (size_t)wn * 8, (size_t)words_of(cols) * 8, (size_t)rows,
+                                        cudaMemcpyDeviceToHost, sout));
+        return MELA_OK;
+    };
     auto run = [&]() -> mela_status {
         MELA_CUDA_TRY(cudaEventRecord(ev_alloc, s));
         MELA_CUDA_TRY(cudaStreamWaitEvent(sin, ev_alloc, 0));
         MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_alloc, 0));
-        // B first: the whole of it is needed by every block
-        MELA_CUDA_TRY(cudaMemcpy2DAsync(bb, (size_t)wn * 8, B, (size_t)ldb * 8, (size_t)wn * 8, (size_t)k,
-                                        cudaMemcpyHostToDevice, s));
-        for (i64 i = 0; i < nblk; ++i) {
-            const i64 r0 = i * brows, rows = (m - r0) < brows ? (m - r0) : brows;
-            MELA_CUDA_TRY(cudaMemcpy2DAsync(a + r0 * wk, (size_t)wk * 8, A + r0 * lda, (size_t)lda * 8,
-                                            (size_t)wk * 8, (size_t)rows, cudaMemcpyHostToDevice, sin));
-            MELA_CUDA_TRY(cudaEventRecord(ev_up(i), sin));
+        for (int r = 0; r < (bm > bn ? bm : bn); ++r) {
+            if (r < bm) {
+                const i64 r0 = r * mb;
+                MELA_CUDA_TRY(cudaMemcpy2DAsync(a + r0 * wk, (size_t)wk * 8, A + r0 * lda, (size_t)lda * 8,
+                                                (size_t)wk * 8, (size_t)rows_of(r), cudaMemcpyHostToDevice, sin));
+                MELA_CUDA_TRY(cudaEventRecord(ev_a(r), sin));
+            }
+            if (r < bn) {
+                const i64 w0 = r * nb / 64;
+                MELA_CUDA_TRY(cudaMemcpy2DAsync(bb + w0, (size_t)wn * 8, B + w0, (size_t)ldb * 8,
+                                                (size_t)words_of(cols_of(r)) * 8, (size_t)k,
+                                                cudaMemcpyHostToDevice, sin));
+                MELA_CUDA_TRY(cudaEventRecord(ev_b(r), sin));
+            }
         }
-        mela_status st2 = launch_transpose(bb, wn, k, n, b.Bt, p.ldbt, s);
-        if (st2 != MELA_OK) return st2;
+        // the pad word of each Bt row must read as zero
         if (p.ldbt > wk) MELA_CUDA_TRY(cudaMemset2DAsync(b.Bt + wk, (size_t)p.ldbt * 8, 0, 8, (size_t)n, s));
-        st2 = fp4 ? launch_expand_f4(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)
-                  : launch_expand_u8(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s);
-        if (st2 != MELA_OK) return st2;
-        for (i64 i = 0; i < nblk; ++i) {
-            const i64 r0 = i * brows, rows = (m - r0) < brows ? (m - r0) : brows;
-            const i64 rp = (rows + 255) / 256 * 256;
-            unsigned char *a8 = b.A8 + (size_t)r0 * p.kp;
-            MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_up(i), 0));
-            st2 = fp4 ? launch_expand_f4(a + r0 * wk, wk, rows, k, rp, p.kp, a8, s)
-                      : launch_expand_u8(a + r0 * wk, wk, rows, k, rp, p.kp, a8, s);
-            if (st2 != MELA_OK) return st2;
-            st2 = launch_gemm_tc(a8, b.B8, rp, p.np, p.kp, c + r0 * wn, wn, rows, n, s, fp4);
-            if (st2 != MELA_OK) return st2;
-            MELA_CUDA_TRY(cudaEventRecord(ev_mul(i), s));
-            MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_mul(i), 0));
-            MELA_CUDA_TRY(cudaMemcpy2DAsync(C + r0 * ldc, (size_t)ldc * 8, c + r0 * wn, (size_t)wn * 8,
-                                            (size_t)wn * 8, (size_t)rows, cudaMemcpyDeviceToHost, sout));
+        mela_status e;
+        for (int r = 0; r < (bm > bn ? bm : bn); ++r) {
+            if (r < bm) {
+                const i64 r0 = r * mb, rows = rows_of(r);
+                MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_a(r), 0));
+                e = fp4 ? launch_expand_f4(a + r0 * wk, wk, rows, k, round_up(rows, 256), p.kp,
+                                           b.A8 + (size_t)r0 * p.kp, s)
+                        : launch_expand_u8(a + r0 * wk, wk, rows, k, round_up(rows, 256), p.kp,
+                                           b.A8 + (size_t)r0 * p.kp, s);
+                if (e != MELA_OK) return e;
+                for (int j = 0; j < r && j < bn; ++j)
+                    if ((e = product(r, j)) != MELA_OK) return e;
+            }
+            if (r < bn) {
+                const i64 c0 = r * nb, cols = cols_of(r);
+                MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_b(r), 0));
+                e = launch_transpose(bb + c0 / 64, wn, k, cols, b.Bt + (size_t)c0 * p.ldbt, p.ldbt, s);
+                if (e != MELA_OK) return e;
+                e = fp4 ? launch_expand_f4(b.Bt + (size_t)c0 * p.ldbt, p.ldbt, cols, k, round_up(cols, 256), p.kp,
+                                           b.B8 + (size_t)c0 * p.kp, s)
+                        : launch_expand_u8(b.Bt + (size_t)c0 * p.ldbt, p.ldbt, cols, k, round_up(cols, 256), p.kp,
+                                           b.B8 + (size_t)c0 * p.kp, s);
+                if (e != MELA_OK) return e;
+                for (int i = 0; i <= r && i < bm; ++i)
+                    if ((e = product(i, r)) != MELA_OK) return e;
+            }
         }
         return MELA_OK;
     };
@@ -541,7 +574,7 @@ extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, c
     if (st != MELA_OK) return st;
     {
         const int v = plan_gemm(variant, m, k, n).variant;
-        if ((v == MELA_GEMM_TC || v == MELA_GEMM_TC_FP4) && k > 0 && m >= 2 * kPipeRows)
+        if ((v == MELA_GEMM_TC || v == MELA_GEMM_TC_FP4) && k > 0 && m >= kPipeMin && n >= kPipeMin)
             return matmul_packed_host_pipelined(A, lda, B, ldb, C, ldc, m, k, n, v, s);
     }
     const i64 wk = words_of(k), wn = words_of(n);

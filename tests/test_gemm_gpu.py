@@ -186,11 +186,12 @@ def test_fp4_variants_agree_large(cuda):
 
 
 @pytest.mark.parametrize("variant", ["tc", "tc_fp4", "plain"])
-@pytest.mark.parametrize("shape", [(9000, 1000, 700), (8192, 64, 65), (20000, 300, 256)])
+@pytest.mark.parametrize("shape", [(9000, 1000, 9000), (8192, 64, 8192), (20000, 300, 8300), (9000, 1000, 700)])
 def test_packed_host_product(cuda, variant, shape):
-    """The host-buffer product (transfers overlapped in row blocks for the
-    tensor-core forms once m >= 8192) equals the device product of the oracle's
-    inputs, including a ragged last block and page-locked and pageable buffers."""
+    """The host-buffer product (for the tensor-core forms once m and n reach
+    8192, transfers overlapped in row blocks of A and column blocks of B) equals
+    the device product of the oracle's inputs, with ragged last blocks (a
+    partial word of columns included) and page-locked and pageable buffers."""
     import torch
     from mex_linear_algebra_b200 import _lib
     m, k, n = shape
