@@ -81,6 +81,7 @@ struct HostCtx {
     cudaStream_t stream[kMaxDevices] = {};
     cudaStream_t copy_in[kMaxDevices] = {};   // pipelined host products: uploads
     cudaStream_t copy_out[kMaxDevices] = {};  //   and downloads
+    cudaStream_t side[kMaxDevices] = {};      // work forked off a caller's stream
 };
 static thread_local HostCtx t_ctx;
 
@@ -113,6 +114,14 @@ static mela_status copy_streams(cudaStream_t *in, cudaStream_t *out)
     if (!t_ctx.copy_out[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.copy_out[d], cudaStreamNonBlocking));
     *in = t_ctx.copy_in[d];
     *out = t_ctx.copy_out[d];
+    return MELA_OK;
+}
+
+mela_status side_stream(cudaStream_t *s)
+{
+    const int d = current_device();
+    if (!t_ctx.side[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.side[d], cudaStreamNonBlocking));
+    *s = t_ctx.side[d];
     return MELA_OK;
 }
 

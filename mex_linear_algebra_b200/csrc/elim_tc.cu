@@ -138,7 +138,8 @@ __device__ __forceinline__ int block_slot(bool flag, int *wsum, int &total)
 // ---------------------------------------------------------------- window_factor
 __global__ void __launch_bounds__(WF_THREADS, 1)
 window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int *list, const unsigned char *live,
-                     unsigned char *state, int *stamp, int wid, WinState *ws, long long *piv, long long *prow)
+                     unsigned char *state, int *stamp, int wid, const WinState *prev, WinState *ws, long long *piv,
+                     long long *prow)
 {
     extern __shared__ __align__(16) unsigned char wf_raw[];
     WfSmem &S = *reinterpret_cast<WfSmem *>(wf_raw);
@@ -147,8 +148,8 @@ window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int
     const int wn = (wc - w) < WW ? (int)(wc - w) : WW;
     const i64 vb = n - 64 * w;
     const int valid = vb < WBITS ? (int)vb : WBITS;  // columns of this window inside the matrix
-    const int na = ws->na;
-    int *L0 = list + ws->lbase;
+    const int na = prev->na;
+    int *L0 = list + prev->lbase;
     constexpr unsigned NOKEY = 0xFFFFFFFFu;
 
     for (int e = tid; e < 64 * 16 * WW; e += WF_THREADS) {
@@ -333,7 +334,7 @@ window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int
 
     // results: pivot t = t-th leading bit; P-index t is its physical row
     const int nb = S.nb;
-    const long long r0 = ws->rank;
+    const long long r0 = prev->rank;
     if (tid < WBITS && ((S.have[tid >> 6] >> (tid & 63)) & 1)) {
         int t = 0;
         for (int q = 0; q < (tid >> 6); ++q) t += __popcll(S.have[q]);
@@ -372,7 +373,7 @@ window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int
     if (tid == 0) {
         ws->rt = nb;
         ws->nu = 0;
-        ws->lbase += S.cnt;  // S.cnt = entries dropped
+        ws->lbase = prev->lbase + S.cnt;  // S.cnt = entries dropped
         ws->na = na - S.cnt;
         ws->rank = r0 + nb;
     }
@@ -590,12 +591,15 @@ struct UCtl {
 __global__ void __launch_bounds__(U_THREADS, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmR,
                  u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const WinState *ws, const int *__restrict__ ulist,
-                 unsigned char *live, u32 *err)
+                 unsigned char *live, int strip_lo, int strip_hi, u32 *err)
 {
+    // strips strip_lo .. strip_hi-1 (256 columns each, from the window's first column)
     const int rt = ws->rt, nu = ws->nu;
     if (rt == 0 || nu == 0) return;
     const i64 lw = wc - w;
-    const int strips = (int)((lw + 3) / 4);
+    const int s_end = (int)((lw + 3) / 4) < strip_hi ? (int)((lw + 3) / 4) : strip_hi;
+    const int strips = s_end - strip_lo;
+    if (strips <= 0) return;
     const int mt = (nu + UM - 1) / UM;
     const int chunks = (mt + U_MCH - 1) / U_MCH;
     const long long units = (long long)strips * chunks;
@@ -653,7 +657,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             for (int q = 0; q < U_BSTAGES; ++q) last_b[q] = -1;
             bool ok = true;
             for (long long u = ub; u < ue && ok; ++u) {
-                const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+                const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
                 if (strip != prev_strip) {
                     const int bs = nbl % U_BSTAGES;
                     if (nbl >= U_BSTAGES && !ptx::mbar_wait(&ctl->bempty[bs], ((nbl / U_BSTAGES) - 1) & 1, err)) {
@@ -705,7 +709,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             int nbl = 0, it = 0, prev_strip = -1, bs = 0;
             bool ok = true;
             for (long long u = ub; u < ue && ok; ++u) {
-                const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+                const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
                 if (strip != prev_strip) {
                     bs = nbl % U_BSTAGES;
                     if (!ptx::mbar_wait(&ctl->bfull[bs], (nbl / U_BSTAGES) & 1, err) || *abort_flag) {
@@ -739,7 +743,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
                 }
                 if (!ok) break;
                 // the strip's buffer is free once this unit's products are done
-                const bool next_same = (u + 1 < ue) && ((int)((u + 1) / chunks) == strip);
+                const bool next_same = (u + 1 < ue) && (strip_lo + (int)((u + 1) / chunks) == strip);
                 if (!next_same) ptx::umma_commit(&ctl->bempty[bs]);
             }
             if (!ok) {
@@ -821,7 +825,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             return good;
         };
         for (long long u = ub; u < ue; ++u) {
-            const int strip = (int)(u / chunks), chunk = (int)(u % chunks);
+            const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
             const i64 w0 = w + (i64)strip * 4;
             const int nw = (wc - w0) < 4 ? (int)(wc - w0) : 4;
             const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
@@ -899,8 +903,8 @@ TcLayout tc_layout(i64 m, i64 n)
     size_t off = 0;
     L.state = off;  off += al256((size_t)m);
     L.stamp = off;  off += al256((size_t)m * 4);
-    L.live = off;   off += al256((size_t)m);
-    L.ws = off;     off += al256(sizeof(WinState));
+    L.live = off;   off += 2 * al256((size_t)m);          // one flag array per window parity
+    L.ws = off;     off += 2 * al256(sizeof(WinState));   // one state per window parity
     L.ulist = off;  off += al256((size_t)m * 4);
     L.list = off;   off += al256((size_t)m * 4);
     L.x8 = off;     off += al256((size_t)L.mpad * WBITS);
@@ -928,13 +932,13 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     unsigned char *b = (unsigned char *)wsp;
     unsigned char *state = b + L.state;
     int *stamp = (int *)(b + L.stamp);
-    WinState *ws = (WinState *)(b + L.ws);
+    WinState *wsv[2] = {(WinState *)(b + L.ws), (WinState *)(b + L.ws + al256(sizeof(WinState)))};
     int *ulist = (int *)(b + L.ulist);
     unsigned char *X8 = b + L.x8;
     unsigned char *Rt8 = b + L.rt8;
     u64 *Rbuf = (u64 *)(b + L.rbuf);
     int *list = (int *)(b + L.list);
-    unsigned char *live = b + L.live;
+    unsigned char *livev[2] = {b + L.live, b + L.live + al256((size_t)m)};
     const i64 wc = words_of(n);
 
     CUtensorMap mx, mr;
@@ -942,12 +946,14 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     if (st != MELA_OK) return st;
     st = make_u8_kmajor_map(&mr, Rt8, L.npad, WBITS, UN);
     if (st != MELA_OK) return st;
+    cudaStream_t s2;
+    if ((st = side_stream(&s2)) != MELA_OK) return st;
 
     MELA_CUDA_TRY(cudaMemsetAsync(state, 1, (size_t)m, s));
     MELA_CUDA_TRY(cudaMemsetAsync(stamp, 0xff, (size_t)m * 4, s));
-    MELA_CUDA_TRY(cudaMemsetAsync(live, 1, (size_t)m, s));
-    MELA_CUDA_TRY(cudaMemsetAsync(ws, 0, sizeof(WinState), s));
-    list_init_kernel<<<grid_for(m), 256, 0, s>>>(list, m, ws);
+    MELA_CUDA_TRY(cudaMemsetAsync(b + L.live, 1, 2 * al256((size_t)m), s));
+    MELA_CUDA_TRY(cudaMemsetAsync(b + L.ws, 0, 2 * al256(sizeof(WinState)), s));
+    list_init_kernel<<<grid_for(m), 256, 0, s>>>(list, m, wsv[1]);  // the state "before" window 0
     const size_t wf_smem = sizeof(WfSmem);
     MELA_CUDA_TRY(cudaFuncSetAttribute(window_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)wf_smem));
@@ -957,24 +963,68 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     const int sms = sm_count();
     const i64 coef_blocks_full = (m + 255) / 256;
     const int coef_blocks = (int)(coef_blocks_full < (i64)sms * 8 ? coef_blocks_full : (i64)sms * 8);
+    const i64 chunks_max = (L.mpad / UM + U_MCH - 1) / U_MCH;
     u32 *err = device_error_word();
-    int wid = 0;
-    for (i64 w = 0; w < wc; w += WW, ++wid) {
-        const i64 lw = wc - w;
-        window_factor_kernel<<<1, WF_THREADS, wf_smem, s>>>(M, ld, m, n, w, list, live, state, stamp, wid, ws, d_piv,
-                                                            d_prow);
-        window_combine_kernel<<<(unsigned)((lw + CB_W - 1) / CB_W), 256, cb_smem, s>>>(
-            M, ld, wc, w, ws, Rbuf, wc);
-        window_coef_kernel<<<coef_blocks, 256, 0, s>>>(M, ld, m, wc, w, list, stamp, wid, rref, ws, ulist, X8, live);
-        window_rt_kernel<<<(unsigned)lw, 256, 0, s>>>(M, ld, w, Rbuf, wc, ws, Rt8);
-        const i64 strips = (lw + 3) / 4;
-        const i64 units_max = strips * ((L.mpad / UM + U_MCH - 1) / U_MCH);
-        const int grid = (int)(units_max < sms ? units_max : sms);
-        tc_update_kernel<<<grid, U_THREADS, U_SMEM, s>>>(mx, mr, M, ld, wc, w, ws, ulist, live, err);
+
+    // Look-ahead: the update of window w is split into its first two strips
+    // (window w itself and window w+1), run on the caller's stream before
+    // window w+1 is factored, and the rest, forked to the side stream so that
+    // it runs while window w+1 is factored (on an SM the fork leaves free).
+    // Window w+1's combine waits for it: it reads the pivot rows' later words,
+    // and its coefficient and R buffers are the ones the rest still reads.
+    // Window states and row flags alternate by window parity so that the
+    // factorization of w+1 never writes what the update of w reads.
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    MELA_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventDestroy(ev_fork);
+        set_error("cudaEventCreate failed");
+        return MELA_ERR_CUDA;
     }
-    MELA_LAUNCH_CHECK("tensor-core elimination");
-    MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &ws->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));
-    return MELA_OK;
+    auto run = [&]() -> mela_status {
+        bool forked = false;
+        int wid = 0;
+        for (i64 w = 0; w < wc; w += WW, ++wid) {
+            const i64 lw = wc - w;
+            WinState *cur = wsv[wid & 1], *prev = wsv[(wid + 1) & 1];
+            unsigned char *live = livev[wid & 1];  // flags of window wid-2 (complete); then this window's
+            window_factor_kernel<<<1, WF_THREADS, wf_smem, s>>>(M, ld, m, n, w, list, live, state, stamp, wid, prev,
+                                                                cur, d_piv, d_prow);
+            if (forked) {
+                MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_join, 0));
+                forked = false;
+            }
+            window_combine_kernel<<<(unsigned)((lw + CB_W - 1) / CB_W), 256, cb_smem, s>>>(M, ld, wc, w, cur, Rbuf,
+                                                                                           wc);
+            window_coef_kernel<<<coef_blocks, 256, 0, s>>>(M, ld, m, wc, w, list, stamp, wid, rref, cur, ulist, X8,
+                                                           live);
+            window_rt_kernel<<<(unsigned)lw, 256, 0, s>>>(M, ld, w, Rbuf, wc, cur, Rt8);
+            const i64 strips = (lw + 3) / 4;
+            const i64 near = strips < 2 ? strips : 2;
+            const int grid_near = (int)(near * chunks_max < sms ? near * chunks_max : sms);
+            tc_update_kernel<<<grid_near, U_THREADS, U_SMEM, s>>>(mx, mr, M, ld, wc, w, cur, ulist, live, 0, 2, err);
+            if (strips > 2) {
+                const i64 units = (strips - 2) * chunks_max;
+                const int cap = sms > 4 ? sms - 2 : sms;  // SMs left for the next factorization
+                const int grid_far = (int)(units < cap ? units : cap);
+                MELA_CUDA_TRY(cudaEventRecord(ev_fork, s));
+                MELA_CUDA_TRY(cudaStreamWaitEvent(s2, ev_fork, 0));
+                tc_update_kernel<<<grid_far, U_THREADS, U_SMEM, s2>>>(mx, mr, M, ld, wc, w, cur, ulist, live, 2,
+                                                                     (int)strips, err);
+                MELA_CUDA_TRY(cudaEventRecord(ev_join, s2));
+                forked = true;
+            }
+        }
+        if (forked) MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_join, 0));
+        MELA_LAUNCH_CHECK("tensor-core elimination");
+        WinState *last = wsv[(wid + 1) & 1];  // the state written by the last window (wid-1)
+        MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &last->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+        return MELA_OK;
+    };
+    st = run();
+    cudaEventDestroy(ev_fork);
+    cudaEventDestroy(ev_join);
+    return st;
 }
 
 }  // namespace mela

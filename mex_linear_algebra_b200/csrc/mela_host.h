@@ -19,6 +19,9 @@ struct DevBuf {
 
 // The calling thread's library stream on the current device.
 mela_status host_stream(cudaStream_t *s);
+// The calling thread's side stream on the current device: work forked from a
+// caller's stream (through an event) and joined back to it before returning.
+mela_status side_stream(cudaStream_t *s);
 // Synchronise `s` and turn a device-side wait timeout into MELA_ERR_TIMEOUT.
 mela_status finish(cudaStream_t s);
 
