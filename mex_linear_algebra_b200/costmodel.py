@@ -128,7 +128,9 @@ def choose(op: str, m: int, n: int, p: int, density: float) -> str:
 def heuristic(op: str, m: int, n: int, p: int, density: float) -> str:
     """The library's fixed rule (what dispatch does without a model)."""
     if op == "matmul":
-        return "tc" if (m >= 1024 and n >= 1024 and p >= 1024) else "plain"
+        if m >= 1024 and n >= 1024 and p >= 1024:
+            return "tc_fp4" if n < (1 << 23) else "tc"
+        return "plain"
     return "fused" if m * n < 65536 else "tc"
 
 

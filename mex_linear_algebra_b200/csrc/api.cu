@@ -183,8 +183,9 @@ int choose_gemm_variant(i64 m, i64 k, i64 n)
         return v;
     }
     // fixed rule: tensor cores pay off once every dimension spans a few
-    // tiles; below that the expansion to bytes dominates
-    if (m >= 1024 && n >= 1024 && k >= 1024) return MELA_GEMM_TC;
+    // tiles (below that the expansion of the operands dominates); the FP4
+    // form runs at twice the INT8 rate while its f32 sums stay exact
+    if (m >= 1024 && n >= 1024 && k >= 1024) return k < (1LL << 23) ? MELA_GEMM_TC_FP4 : MELA_GEMM_TC;
     return MELA_GEMM_PLAIN;
 }
 
