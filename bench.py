@@ -582,6 +582,39 @@ def run_mela(args, ws, rank, local):
     return 0 if ok else 1
 
 
+def elim_only():
+    """One rank and one RREF of the 16384 x 32768 rank-12000 configuration by the
+    tensor-core elimination form (the dense section's inputs), for profiling."""
+    import torch
+    from mex_linear_algebra_b200 import device as D, gen, _lib
+    from mex_linear_algebra_b200._lib import check, lib
+    m, r0, n = 16384, 12000, 32768
+    A = D.matmul(D.rand_dense(2, 0, m, r0), D.rand_dense(2, 1, r0, n), m, r0, n, variant="tc")
+    for (i, a, b) in gen.replacement_triples(m, 164):
+        A[i] = A[a] ^ A[b]
+    L = lib()
+    s = torch.cuda.current_stream().cuda_stream
+    wc = n // 64
+    wsb = L.mela_elim_workspace_size(m, n)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    dpv = torch.empty(m, dtype=torch.int64, device="cuda")
+    dpr = torch.empty(m, dtype=torch.int64, device="cuda")
+    out = {}
+    for name, fn in (("rank", L.mela_dev_rank), ("rref", L.mela_dev_rref)):
+        Mx = A.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        check(fn(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                 ws.data_ptr(), wsb, s))
+        e1.record()
+        e1.synchronize()
+        out[name + "_ms"] = round(e0.elapsed_time(e1), 3)
+        out[name] = int(dr.item())
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,8 +629,13 @@ def main():
                     help="skip the batched / dense-rank / dispatch sections")
     ap.add_argument("--variant", choices=["tc", "tc_fp4"], default="tc_fp4",
                     help="tensor-core form timed as the headline (both are reported)")
+    ap.add_argument("--elim-only", action="store_true",
+                    help="profiling aid: build the dense rank configuration and run one rank and one "
+                         "RREF with the tensor-core elimination form, print their times, nothing else")
     args = ap.parse_args()
     set_size(args.size)
+    if args.elim_only:
+        return elim_only()
     from mex_linear_algebra_b200 import parallel
     ws, rank, local = parallel.world()
     if args.impl == "reference":
