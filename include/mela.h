@@ -128,6 +128,29 @@ mela_status mela_null_gf2(const mela_host_matrix *H, mela_alloc_fn alloc, void *
 mela_status mela_null_m4ri(const mela_host_matrix *H, mela_alloc_fn alloc, void *ctx,
                            int64_t *nullity);
 
+/* Sparse input.  No counterpart in the reference, whose gateways reject
+ * sparse arrays or read their values as if dense.  MATLAB's own layout:
+ * column j holds entries colptr[j] .. colptr[j+1]-1 (colptr[0] = 0,
+ * non-decreasing) with 0-based rows rowidx[e] (MATLAB's jc / ir); values is
+ * NULL (every entry 1) or one logical byte / double per entry (a double read
+ * as ((int)x) & 1, like dense input).  Repeated (row, column) entries add
+ * mod 2.  Bad pointers or indices -> MELA_ERR_INVALID (checked on the host
+ * before any device work). */
+typedef struct {
+    int32_t kind; /* MELA_KIND_LOGICAL or MELA_KIND_DOUBLE: the type of values */
+    int64_t rows;
+    int64_t cols;
+    const int64_t *colptr; /* cols + 1 entries */
+    const int64_t *rowidx; /* colptr[cols] entries */
+    const void *values;    /* NULL or colptr[cols] entries */
+} mela_host_csc;
+/* Rank over GF(2) of a sparse matrix (the same result as mela_rank_gf2 on
+ * its dense form; the elimination variant is chosen by the dispatcher). */
+mela_status mela_rank_csc(const mela_host_csc *H, int64_t *rank);
+/* Null-space basis of a sparse matrix: the output of mela_null_gf2 on its
+ * dense form (n x nullity logical, column-major, through `alloc`). */
+mela_status mela_null_csc(const mela_host_csc *H, mela_alloc_fn alloc, void *ctx, int64_t *nullity);
+
 /* ------------------------------------------------------------------ */
 /* gateway semantics (shared by the MEX files and other front ends)     */
 /* ------------------------------------------------------------------ */
@@ -180,6 +203,12 @@ mela_status mela_dev_rand_bernoulli(uint64_t seed, uint64_t stream_id, int64_t m
  * and the inline packs of the other gateways. */
 mela_status mela_dev_pack(int32_t kind, int64_t m, int64_t n, const void *d_in,
                           uint64_t *d_out, int64_t ld, void *stream);
+/* Sparse (CSC, device arrays; see mela_host_csc) -> packed rows.  Row
+ * indices outside [0, m) are skipped and flagged in the device error word
+ * (mela_device_error_flags). */
+mela_status mela_dev_pack_csc(const int64_t *d_colptr, const int64_t *d_rowidx, const void *d_values,
+                              int32_t kind, int64_t m, int64_t n, uint64_t *d_out, int64_t ld,
+                              void *stream);
 /* Packed rows -> column-major logical bytes (src/mela_matmul_gf2.c:193-205). */
 mela_status mela_dev_unpack(const uint64_t *d_in, int64_t ld, int64_t m, int64_t n,
                             uint8_t *d_out, void *stream);

@@ -52,6 +52,11 @@ class HostMatrix(C.Structure):
                 ("cols", C.c_int64), ("data", C.c_void_p)]
 
 
+class HostCsc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("rows", C.c_int64), ("cols", C.c_int64),
+                ("colptr", C.c_void_p), ("rowidx", C.c_void_p), ("values", C.c_void_p)]
+
+
 # name -> (restype, argtypes); the list of every exported entry point
 _i64, _u64, _i32, _u32, _vp, _sz = C.c_int64, C.c_uint64, C.c_int32, C.c_uint32, C.c_void_p, C.c_size_t
 _st = C.c_int
@@ -66,6 +71,9 @@ SIGNATURES = {
     "mela_rank_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(C.c_double)]),
     "mela_null_gf2": (_st, [C.POINTER(HostMatrix), ALLOC_FN, _vp, C.POINTER(_i64)]),
     "mela_null_m4ri": (_st, [C.POINTER(HostMatrix), ALLOC_FN, _vp, C.POINTER(_i64)]),
+    "mela_rank_csc": (_st, [C.POINTER(HostCsc), C.POINTER(_i64)]),
+    "mela_null_csc": (_st, [C.POINTER(HostCsc), ALLOC_FN, _vp, C.POINTER(_i64)]),
+    "mela_dev_pack_csc": (_st, [_vp, _vp, _vp, _i32, _i64, _i64, _vp, _i64, _vp]),
     "mela_gateway": (C.c_int, [_i32, _i32, _i32, C.POINTER(HostMatrix), GATEWAY_ALLOC_FN, _vp,
                                C.POINTER(GatewayError)]),
     "mela_matmul_packed_host": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i32]),

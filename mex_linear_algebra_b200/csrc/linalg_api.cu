@@ -12,6 +12,71 @@ namespace mela {
 
 static bool ok_kind(int k) { return k == MELA_KIND_LOGICAL || k == MELA_KIND_DOUBLE; }
 
+// Rank of a packed device matrix (overwritten), read back to the host.
+mela_status rank_of_packed(u64 *P, i64 ld, i64 m, i64 n, int variant, cudaStream_t s, double *rank)
+{
+    const i64 mn = m < n ? m : n;
+    DevBuf ws, out;
+    mela_status st;
+    const size_t wsb = elim_workspace(m, n);
+    if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
+    if ((st = out.alloc((size_t)(1 + 2 * mn) * 8, s)) != MELA_OK) return st;
+    long long *d = (long long *)out.p;
+    st = elim_device(variant, P, ld, m, n, 0, d, d + 1, d + 1 + mn, ws.p, wsb, s);
+    if (st != MELA_OK) return st;
+    long long r = 0;
+    MELA_CUDA_TRY(cudaMemcpyAsync(&r, d, sizeof r, cudaMemcpyDeviceToHost, s));
+    if ((st = finish(s)) != MELA_OK) return st;
+    *rank = (double)r;
+    return MELA_OK;
+}
+
+// Null-space basis of a packed device matrix (overwritten by its RREF) into
+// the caller's n x nullity logical buffer from `alloc`.  m may be 0.
+mela_status null_of_packed(u64 *P, i64 ld, i64 m, i64 n, int variant, mela_alloc_fn alloc, void *ctx,
+                           int64_t *nullity, cudaStream_t s)
+{
+    if (n == 0) {
+        if (nullity) *nullity = 0;
+        alloc(ctx, 0, 0);  // an empty n x 0 result; the buffer is not written
+        return MELA_OK;
+    }
+    const i64 mn = m < n ? m : n;
+    mela_status st;
+    DevBuf ws, out;
+    if ((st = out.alloc((size_t)(1 + 2 * (mn ? mn : 1)) * 8, s)) != MELA_OK) return st;
+    long long *d = (long long *)out.p;
+    long long r = 0;
+    if (m > 0) {
+        const size_t wsb = elim_workspace(m, n);
+        if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
+        st = elim_device(variant, P, ld, m, n, 1, d, d + 1, d + 1 + mn, ws.p, wsb, s);
+        if (st != MELA_OK) return st;
+        MELA_CUDA_TRY(cudaMemcpyAsync(&r, d, sizeof r, cudaMemcpyDeviceToHost, s));
+        MELA_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    const i64 f = n - r;
+    uint8_t *Z = alloc(ctx, n, f);
+    if (!Z && f > 0) {
+        set_error("output allocation failed");
+        return MELA_ERR_NOMEM;
+    }
+    if (nullity) *nullity = f;
+    if (f == 0) return finish(s);
+    const i64 ldz = even_words(n);
+    DevBuf Zt, nws, bytes;
+    if ((st = Zt.alloc((size_t)f * ldz * 8, s)) != MELA_OK) return st;
+    const NullLayout NL = null_layout(n, r);
+    if ((st = nws.alloc(NL.total, s)) != MELA_OK) return st;
+    st = null_basis_device((const u64 *)P, ld, m, n, r, d + 1, d + 1 + mn, (u64 *)Zt.p, ldz, nws.p, NL.total, s);
+    if (st != MELA_OK) return st;
+    if ((st = bytes.alloc((size_t)f * n, s)) != MELA_OK) return st;
+    if ((st = launch_unpack_rows((const u64 *)Zt.p, ldz, f, n, (unsigned char *)bytes.p, s)) != MELA_OK)
+        return st;
+    MELA_CUDA_TRY(cudaMemcpyAsync(Z, bytes.p, (size_t)f * n, cudaMemcpyDeviceToHost, s));
+    return finish(s);
+}
+
 mela_status host_rank(const mela_host_matrix *A, int variant, double *rank)
 {
     if (!A || !rank) {
@@ -33,21 +98,10 @@ mela_status host_rank(const mela_host_matrix *A, int variant, double *rank)
     mela_status st = host_stream(&s);
     if (st != MELA_OK) return st;
     const i64 ld = even_words(n);
-    const i64 mn = m < n ? m : n;
-    DevBuf P, stage, ws, out;
+    DevBuf P, stage;
     if ((st = P.alloc((size_t)m * ld * 8, s)) != MELA_OK) return st;
     if ((st = upload_and_pack(A, (u64 *)P.p, ld, s, stage)) != MELA_OK) return st;
-    const size_t wsb = elim_workspace(m, n);
-    if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
-    if ((st = out.alloc((size_t)(1 + 2 * mn) * 8, s)) != MELA_OK) return st;
-    long long *d = (long long *)out.p;
-    st = elim_device(variant, (u64 *)P.p, ld, m, n, 0, d, d + 1, d + 1 + mn, ws.p, wsb, s);
-    if (st != MELA_OK) return st;
-    long long r = 0;
-    MELA_CUDA_TRY(cudaMemcpyAsync(&r, d, sizeof r, cudaMemcpyDeviceToHost, s));
-    if ((st = finish(s)) != MELA_OK) return st;
-    *rank = (double)r;
-    return MELA_OK;
+    return rank_of_packed((u64 *)P.p, ld, m, n, variant, s, rank);
 }
 
 mela_status host_null(const mela_host_matrix *H, int variant, mela_alloc_fn alloc, void *ctx,
@@ -74,42 +128,10 @@ mela_status host_null(const mela_host_matrix *H, int variant, mela_alloc_fn allo
     mela_status st = host_stream(&s);
     if (st != MELA_OK) return st;
     const i64 ld = even_words(n);
-    const i64 mn = m < n ? m : n;
-    DevBuf P, stage, ws, out;
+    DevBuf P, stage;
     if ((st = P.alloc((size_t)(m ? m : 1) * ld * 8, s)) != MELA_OK) return st;
-    if ((st = out.alloc((size_t)(1 + 2 * (mn ? mn : 1)) * 8, s)) != MELA_OK) return st;
-    long long *d = (long long *)out.p;
-    long long r = 0;
-    if (m > 0) {
-        if ((st = upload_and_pack(H, (u64 *)P.p, ld, s, stage)) != MELA_OK) return st;
-        const size_t wsb = elim_workspace(m, n);
-        if ((st = ws.alloc(wsb, s)) != MELA_OK) return st;
-        st = elim_device(variant, (u64 *)P.p, ld, m, n, 1, d, d + 1, d + 1 + mn, ws.p, wsb, s);
-        if (st != MELA_OK) return st;
-        MELA_CUDA_TRY(cudaMemcpyAsync(&r, d, sizeof r, cudaMemcpyDeviceToHost, s));
-        MELA_CUDA_TRY(cudaStreamSynchronize(s));
-    }
-    const i64 f = n - r;
-    uint8_t *Z = alloc(ctx, n, f);
-    if (!Z && f > 0) {
-        set_error("output allocation failed");
-        return MELA_ERR_NOMEM;
-    }
-    if (nullity) *nullity = f;
-    if (f == 0) return finish(s);
-    const i64 ldz = even_words(n);
-    DevBuf Zt, nws, bytes;
-    if ((st = Zt.alloc((size_t)f * ldz * 8, s)) != MELA_OK) return st;
-    const NullLayout NL = null_layout(n, r);
-    if ((st = nws.alloc(NL.total, s)) != MELA_OK) return st;
-    st = null_basis_device((const u64 *)P.p, ld, m, n, r, d + 1, d + 1 + mn, (u64 *)Zt.p, ldz, nws.p,
-                           NL.total, s);
-    if (st != MELA_OK) return st;
-    if ((st = bytes.alloc((size_t)f * n, s)) != MELA_OK) return st;
-    if ((st = launch_unpack_rows((const u64 *)Zt.p, ldz, f, n, (unsigned char *)bytes.p, s)) != MELA_OK)
-        return st;
-    MELA_CUDA_TRY(cudaMemcpyAsync(Z, bytes.p, (size_t)f * n, cudaMemcpyDeviceToHost, s));
-    return finish(s);
+    if (m > 0 && (st = upload_and_pack(H, (u64 *)P.p, ld, s, stage)) != MELA_OK) return st;
+    return null_of_packed((u64 *)P.p, ld, m, n, variant, alloc, ctx, nullity, s);
 }
 
 }  // namespace mela

@@ -40,6 +40,12 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
 mela_status gemm_device(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                         i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s);
 
+// Rank / null-space basis of a packed device matrix (overwritten), shared by
+// the dense and sparse host entry points.
+mela_status rank_of_packed(u64 *P, i64 ld, i64 m, i64 n, int variant, cudaStream_t s, double *rank);
+mela_status null_of_packed(u64 *P, i64 ld, i64 m, i64 n, int variant, mela_alloc_fn alloc, void *ctx,
+                           int64_t *nullity, cudaStream_t s);
+
 // Copy a host MATLAB array to the device and pack it into dP (ld words/row).
 mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStream_t s,
                             DevBuf &staging);

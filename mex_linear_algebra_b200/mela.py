@@ -104,6 +104,61 @@ def mela_null_m4ri(H):
     return _call(_lib.FN_NULL_M4RI, (H,))
 
 
+# ---------------------------------------------------------------- sparse input
+# No counterpart in the reference (its gateways reject sparse arrays): rank and
+# null space of a sparse matrix packed on the GPU from its CSC arrays.
+
+def _host_csc(H, keep: list):
+    """scipy.sparse matrix, or a tuple (colptr, rowidx, values or None, (rows, cols))."""
+    if hasattr(H, "tocsc"):
+        H = H.tocsc()
+        colptr, rowidx, values, shape = H.indptr, H.indices, H.data, H.shape
+    else:
+        colptr, rowidx, values, shape = H
+    colptr = np.ascontiguousarray(colptr, dtype=np.int64)
+    rowidx = np.ascontiguousarray(rowidx, dtype=np.int64)
+    kind = _lib.KIND_LOGICAL
+    if values is not None:
+        values = np.asarray(values)
+        if values.dtype == np.bool_:
+            values = np.ascontiguousarray(values.view(np.uint8))
+        else:
+            values = np.ascontiguousarray(values, dtype=np.float64)
+            kind = _lib.KIND_DOUBLE
+    keep.extend([colptr, rowidx, values])
+    return _lib.HostCsc(kind, int(shape[0]), int(shape[1]), colptr.ctypes.data,
+                        rowidx.ctypes.data if rowidx.size else None,
+                        values.ctypes.data if values is not None and values.size else None)
+
+
+def rank_csc(H) -> int:
+    """Rank over GF(2) of a sparse matrix (scipy.sparse, or (colptr, rowidx,
+    values, shape)); entries add mod 2, doubles read as ((int)x) & 1."""
+    keep: list = []
+    h = _host_csc(H, keep)
+    r = C.c_int64(0)
+    _lib.check(lib().mela_rank_csc(C.byref(h), C.byref(r)))
+    return int(r.value)
+
+
+def null_csc(H):
+    """n x nullity logical null-space basis of a sparse matrix (the basis
+    mela_null_gf2 returns for its dense form)."""
+    keep: list = []
+    h = _host_csc(H, keep)
+    out = {}
+
+    def alloc(ctx, rows, cols):
+        a = np.zeros((rows, cols), dtype=np.bool_, order="F")
+        out["z"] = a
+        return a.ctypes.data if a.size else None
+
+    cb = _lib.ALLOC_FN(alloc)
+    f = C.c_int64(0)
+    _lib.check(lib().mela_null_csc(C.byref(h), cb, None, C.byref(f)))
+    return out["z"]
+
+
 def call(name: str, *args, nlhs: int = 1):
     """Call a gateway by its MATLAB name with explicit argument counts
     (for reproducing argument-count errors)."""
