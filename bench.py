@@ -2,13 +2,14 @@
 """Benchmark: GF(2) GEMM Tbitop/s at 32768^3; batched rank+null mats/s.
 
 Headline (value): C = A*B over GF(2) with A, B 32768 x 32768, iid
-Bernoulli(1/2) from seed 1, packed uint64 row-major, by the tcgen05 kind::i8
-tensor-core form (operand preparation -- transpose of B and 0/1 byte
-expansion -- plus the tensor-core kernel).  Bit-ops are counted as 2*m*n*k
-(one AND and one XOR per term), the analogue of 2mnk FLOPs.
+Bernoulli(1/2) from seed 1, packed uint64 row-major, by the FP4 tensor-core
+form (tcgen05 kind::mxf4 on CTA pairs; --variant tc for the INT8 form):
+operand preparation -- expansion of A and transposing expansion of B into
+K-major e2m1 values -- plus the tensor-core kernel.  Bit-ops are counted as
+2*m*n*k (one AND and one XOR per term), the analogue of 2mnk FLOPs.
 
   value  -- device-timed (CUDA events, max over ranks) with packed inputs
-            resident in HBM; inputs are 256 MiB packed + 2 GiB of expanded
+            resident in HBM; inputs are 256 MiB packed + 1 GiB of expanded
             operands per step, all larger than L2 (126 MB).
   e2e    -- the same product through the C ABI host entry point
             mela_matmul_packed_host with pinned host buffers: host->device copy
@@ -546,7 +547,7 @@ def run_mela(args, ws, rank, local):
                        "variant": {"tc": "tc (tcgen05 kind::i8)",
                                    "tc_fp4": "tc_fp4 (tcgen05 kind::mxf4, e2m1 0/1, unit scales)"}[args.variant],
                        "seed": SEED,
-                       "l2": "inputs larger than L2 (256 MiB packed + 2 GiB expanded operands)",
+                       "l2": "inputs larger than L2 (256 MiB packed + %s expanded operands)" % ("1 GiB" if args.variant == "tc_fp4" else "2 GiB"),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "result_check": "ok" if ok else "MISMATCH"},
             "roofline": {"bound": "tensor", "achieved": round(achieved, 1), "peak": round(peak, 1),
@@ -568,7 +569,7 @@ def run_mela(args, ws, rank, local):
                              "sample": f"reference mela_matmul_gf2 ({isa}) on A {ms_}x{ks_} * B "
                                        f"{ks_}x{ns_}, one call"},
             "e2e": e2e,
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": 3 * args.steps,  # expand A, transposing expand of B, product
             "forms": forms,
             "clocks": clk,
             "device_error_flags": flags,

@@ -195,8 +195,7 @@ static GemmPlan plan_gemm(int variant, i64 m, i64 k, i64 n)
     if (variant == MELA_GEMM_AUTO) variant = choose_gemm_variant(m, k, n);
     p.variant = variant;
     p.ldbt = even_words(k);
-    if (variant == MELA_GEMM_PLAIN || variant == MELA_GEMM_TC || variant == MELA_GEMM_TC_FP4)
-        p.bt_bytes = (size_t)n * p.ldbt * 8;
+    if (variant == MELA_GEMM_PLAIN) p.bt_bytes = (size_t)n * p.ldbt * 8;
     if (variant == MELA_GEMM_TC) {
         p.mp = round_up(m, 256);  // 256-row tiles for CTA pairs
         p.np = round_up(n, 256);
@@ -255,7 +254,7 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
         set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
         return MELA_ERR_UNSUPPORTED;
     }
-    if (p.variant == MELA_GEMM_PLAIN || p.variant == MELA_GEMM_TC || p.variant == MELA_GEMM_TC_FP4) {
+    if (p.variant == MELA_GEMM_PLAIN) {
         if ((st = launch_transpose(B, ldb, k, n, b.Bt, p.ldbt, s)) != MELA_OK) return st;
         if (p.ldbt > words_of(k)) {
             // the pad word of each Bt row must read as zero
@@ -264,11 +263,11 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
     }
     if (p.variant == MELA_GEMM_TC) {
         if ((st = launch_expand_u8(A, lda, m, k, p.mp, p.kp, b.A8, s)) != MELA_OK) return st;
-        if ((st = launch_expand_u8(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)) != MELA_OK) return st;
+        if ((st = launch_expand_t(B, ldb, k, n, p.np, p.kp, b.B8, false, s)) != MELA_OK) return st;
     }
     if (p.variant == MELA_GEMM_TC_FP4) {
         if ((st = launch_expand_f4(A, lda, m, k, p.mp, p.kp, b.A8, s)) != MELA_OK) return st;
-        if ((st = launch_expand_f4(b.Bt, p.ldbt, n, k, p.np, p.kp, b.B8, s)) != MELA_OK) return st;
+        if ((st = launch_expand_t(B, ldb, k, n, p.np, p.kp, b.B8, true, s)) != MELA_OK) return st;
     }
     return MELA_OK;
 }
@@ -529,8 +528,6 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
                 MELA_CUDA_TRY(cudaEventRecord(ev_b(r), sin));
             }
         }
-        // the pad word of each Bt row must read as zero
-        if (p.ldbt > wk) MELA_CUDA_TRY(cudaMemset2DAsync(b.Bt + wk, (size_t)p.ldbt * 8, 0, 8, (size_t)n, s));
         mela_status e;
         for (int r = 0; r < (bm > bn ? bm : bn); ++r) {
             if (r < bm) {
@@ -547,12 +544,8 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
             if (r < bn) {
                 const i64 c0 = r * nb, cols = cols_of(r);
                 MELA_CUDA_TRY(cudaStreamWaitEvent(s, ev_b(r), 0));
-                e = launch_transpose(bb + c0 / 64, wn, k, cols, b.Bt + (size_t)c0 * p.ldbt, p.ldbt, s);
-                if (e != MELA_OK) return e;
-                e = fp4 ? launch_expand_f4(b.Bt + (size_t)c0 * p.ldbt, p.ldbt, cols, k, round_up(cols, 256), p.kp,
-                                           b.B8 + (size_t)c0 * p.kp, s)
-                        : launch_expand_u8(b.Bt + (size_t)c0 * p.ldbt, p.ldbt, cols, k, round_up(cols, 256), p.kp,
-                                           b.B8 + (size_t)c0 * p.kp, s);
+                e = launch_expand_t(bb + c0 / 64, wn, k, cols, round_up(cols, 256), p.kp, b.B8 + (size_t)c0 * p.kp,
+                                    fp4, s);
                 if (e != MELA_OK) return e;
                 for (int i = 0; i <= r && i < bm; ++i)
                     if ((e = product(i, r)) != MELA_OK) return e;

@@ -19,6 +19,11 @@ mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *
                              cudaStream_t s);
 mela_status launch_expand_f4(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad_bytes,
                              unsigned char *out, cudaStream_t s);
+// Column j of the packed kbits x cols matrix `in` as row j of a K-major
+// tensor-core operand (cols_pad rows, a multiple of 256; kpad bytes per row:
+// 0/1 bytes, or e2m1 pairs when fp4), zero past kbits and cols.
+mela_status launch_expand_t(const u64 *in, i64 ld, i64 kbits, i64 cols, i64 cols_pad, i64 kpad,
+                            unsigned char *out, bool fp4, cudaStream_t s);
 mela_status launch_expand_u8(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 rows_pad, i64 kpad,
                              unsigned char *out, cudaStream_t s);
 

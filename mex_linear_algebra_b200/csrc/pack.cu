@@ -221,6 +221,77 @@ __global__ void __launch_bounds__(256) expand_f4_kernel(const u64 *__restrict__ 
     }
 }
 
+// Transposing expansion: out row j (j < cols_pad) holds column j of the packed
+// kbits x cols matrix `in` as K-major tensor-core values -- 0/1 bytes (F4 =
+// false, kpad bytes per row) or e2m1 pairs (F4 = true, kpad bytes per row =
+// two values each) -- zero past kbits and past cols.  It replaces a bit
+// transpose followed by an expansion.  Block: 256 k x 256 columns.  The
+// 256 x 4-word input tile is read with 32 contiguous bytes per row; each warp
+// turns its 32 rows into 32-bit column slices by ballots; the output rows
+// are written in 16-byte pieces, contiguous along k.
+template <bool F4>
+__global__ void __launch_bounds__(256) expand_t_kernel(const u64 *__restrict__ in, i64 ld, i64 kbits, i64 cols,
+                                                       i64 kpad, unsigned char *__restrict__ out)
+{
+    __shared__ u64 T[256][5];
+    __shared__ u32 U[256][9];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const i64 j0 = (i64)blockIdx.x * 256, k0 = (i64)blockIdx.y * 256;
+    const i64 wc = words_of(cols);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = (tid >> 2) + 64 * i, c = tid & 3;
+        const i64 k = k0 + r, w = (j0 >> 6) + c;
+        T[r][c] = (k < kbits && w < wc) ? in[k * ld + w] : 0ull;
+    }
+    __syncthreads();
+    // warp: k rows 32*warp .. +31; lane keeps the slices of columns lane + 32 g
+    const int r = 32 * warp + lane;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const u64 x = T[r][c];
+        u32 keep0 = 0, keep1 = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+            const u32 v0 = __ballot_sync(0xffffffffu, (u32)(x >> b) & 1u);
+            const u32 v1 = __ballot_sync(0xffffffffu, (u32)(x >> (b + 32)) & 1u);
+            if (lane == b) {
+                keep0 = v0;
+                keep1 = v1;
+            }
+        }
+        U[64 * c + lane][warp] = keep0;
+        U[64 * c + 32 + lane][warp] = keep1;
+    }
+    __syncthreads();
+    if (F4) {
+        // column j, k slice q (32 values): 16 bytes, value k in nibble k & 1 of byte k / 2
+        for (int e = tid; e < 256 * 8; e += 256) {
+            const int j = e >> 3, q = e & 7;
+            const i64 kb = (k0 + 32 * q) / 2;  // byte offset in the output row
+            if (kb >= kpad) continue;
+            const u32 v = U[j][q];
+            u32 o[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const u32 x = (v >> (8 * h)) & 0xFFu;
+                o[h] = (spread_even4(x & 0x55u) << 1) | (spread_even4((x >> 1) & 0x55u) << 5);
+            }
+            *reinterpret_cast<uint4 *>(out + (j0 + j) * kpad + kb) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+    } else {
+        // column j, k slice q (16 values): 16 bytes of 0/1
+        for (int e = tid; e < 256 * 16; e += 256) {
+            const int j = e >> 4, q = e & 15;
+            const i64 kb = k0 + 16 * q;
+            if (kb >= kpad) continue;
+            const u32 h = (U[j][q >> 1] >> (16 * (q & 1))) & 0xFFFFu;
+            *reinterpret_cast<uint4 *>(out + (j0 + j) * kpad + kb) =
+                make_uint4(spread4(h & 15), spread4((h >> 4) & 15), spread4((h >> 8) & 15), spread4((h >> 12) & 15));
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static int grid_for(i64 total, int threads)
 {
@@ -246,6 +317,24 @@ mela_status launch_expand_f4(const u64 *in, i64 ld, i64 rows, i64 kbits, i64 row
     i64 total = rows_pad * (kpad_bytes >> 5);
     expand_f4_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, ld, rows, kbits, rows_pad, kpad_bytes, out);
     MELA_LAUNCH_CHECK("expand_f4_kernel");
+    return MELA_OK;
+}
+
+mela_status launch_expand_t(const u64 *in, i64 ld, i64 kbits, i64 cols, i64 cols_pad, i64 kpad,
+                            unsigned char *out, bool fp4, cudaStream_t s)
+{
+    if (cols_pad <= 0 || kpad <= 0) return MELA_OK;
+    if (cols_pad % 256) {
+        set_error("expand_t: padded column count %lld is not a multiple of 256", cols_pad);
+        return MELA_ERR_INVALID;
+    }
+    const i64 kvals = fp4 ? 2 * kpad : kpad;
+    dim3 grid((unsigned)(cols_pad / 256), (unsigned)((kvals + 255) / 256));
+    if (fp4)
+        expand_t_kernel<true><<<grid, 256, 0, s>>>(in, ld, kbits, cols, kpad, out);
+    else
+        expand_t_kernel<false><<<grid, 256, 0, s>>>(in, ld, kbits, cols, kpad, out);
+    MELA_LAUNCH_CHECK("expand_t_kernel");
     return MELA_OK;
 }
 

@@ -73,6 +73,10 @@ def test_workspace_sizes():
     from mex_linear_algebra_b200 import _lib
     L = _lib.lib()
     assert L.mela_matmul_workspace_size(_lib.GEMM_M4RI, 100, 100, 100) == 0
-    # tensor-core form: transposed B + byte operands padded to the tile grid
+    # INT8 tensor-core form: one byte per bit of both operands, padded to the tile grid
+    # (B is expanded straight from its packed rows, so no transposed copy is kept)
     ws = L.mela_matmul_workspace_size(_lib.GEMM_TC, 32768, 32768, 32768)
-    assert ws >= 2 * 32768 * 32768 + 32768 * 512 * 8
+    assert 2 * 32768 * 32768 <= ws < 2 * 32768 * 32768 + 32768 * 512 * 8
+    # FP4 form: half a byte per bit
+    ws4 = L.mela_matmul_workspace_size(_lib.GEMM_TC_FP4, 32768, 32768, 32768)
+    assert 32768 * 32768 <= ws4 < ws

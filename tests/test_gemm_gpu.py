@@ -209,3 +209,18 @@ def test_packed_host_product(cuda, variant, shape):
                                                       m, k, n, _lib.GEMM_VARIANTS[variant]))
         got = hC.numpy().view(np.uint64)
         assert np.array_equal(valid_words(got, n), valid_words(want, n)), (variant, pinned)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (300, 77, 513), (129, 1000, 300), (64, 256, 256), (200, 5000, 700)])
+def test_tensor_core_forms_odd_shapes(cuda, shape):
+    """Both tensor-core forms (B prepared by the transposing expansion) on
+    shapes that leave partial words, partial 256-column tiles and partial
+    K steps."""
+    D = _dev()
+    m, k, n = shape
+    A = O.rand_dense(71, m + k, m, k)
+    B = O.rand_dense(71, k + n, k, n)
+    want = O.matmul(A, B, m, k, n)
+    for variant in ("tc", "tc_fp4"):
+        got = to_host(D.matmul(to_dev(A), to_dev(B), m, k, n, variant=variant))
+        assert np.array_equal(valid_words(got, n), valid_words(want, n)), variant
