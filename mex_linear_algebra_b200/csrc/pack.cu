@@ -225,44 +225,48 @@ __global__ void __launch_bounds__(256) expand_f4_kernel(const u64 *__restrict__ 
 // kbits x cols matrix `in` as K-major tensor-core values -- 0/1 bytes (F4 =
 // false, kpad bytes per row) or e2m1 pairs (F4 = true, kpad bytes per row =
 // two values each) -- zero past kbits and past cols.  It replaces a bit
-// transpose followed by an expansion.  Block: 256 k x 256 columns.  The
-// 256 x 4-word input tile is read with 32 contiguous bytes per row; each warp
-// turns its 32 rows into 32-bit column slices by ballots; the output rows
+// transpose followed by an expansion.  Block: 256 k x 256 columns.  Each
+// warp reads 32 rows of 256 bits (a lane per row) and turns them into
+// 32-bit column slices by five rounds of shuffle butterflies; the output rows
 // are written in 16-byte pieces, contiguous along k.
 template <bool F4>
 __global__ void __launch_bounds__(256) expand_t_kernel(const u64 *__restrict__ in, i64 ld, i64 kbits, i64 cols,
                                                        i64 kpad, unsigned char *__restrict__ out)
 {
-    __shared__ u64 T[256][5];
     __shared__ u32 U[256][9];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const i64 j0 = (i64)blockIdx.x * 256, k0 = (i64)blockIdx.y * 256;
-    const i64 wc = words_of(cols);
+    // lane = row k0 + 32 warp + lane; a[g] = its 32 bits of columns j0 + 32 g ...
+    const u32 *in32 = reinterpret_cast<const u32 *>(in);
+    const i64 k = k0 + 32 * warp + lane;
+    u32 a[8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int r = (tid >> 2) + 64 * i, c = tid & 3;
-        const i64 k = k0 + r, w = (j0 >> 6) + c;
-        T[r][c] = (k < kbits && w < wc) ? in[k * ld + w] : 0ull;
-    }
-    __syncthreads();
-    // warp: k rows 32*warp .. +31; lane keeps the slices of columns lane + 32 g
-    const int r = 32 * warp + lane;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const u64 x = T[r][c];
-        u32 keep0 = 0, keep1 = 0;
-#pragma unroll
-        for (int b = 0; b < 32; ++b) {
-            const u32 v0 = __ballot_sync(0xffffffffu, (u32)(x >> b) & 1u);
-            const u32 v1 = __ballot_sync(0xffffffffu, (u32)(x >> (b + 32)) & 1u);
-            if (lane == b) {
-                keep0 = v0;
-                keep1 = v1;
-            }
+    for (int g = 0; g < 8; ++g) {
+        const i64 c = j0 + 32 * g;  // first column of word g
+        u32 v = 0;
+        if (k < kbits && c < cols) {
+            v = in32[k * 2 * ld + (c >> 5)];
+            if (cols - c < 32) v &= (1u << (cols - c)) - 1u;
         }
-        U[64 * c + lane][warp] = keep0;
-        U[64 * c + 32 + lane][warp] = keep1;
+        a[g] = v;
     }
+    // 32 x 32 bit transposes across the warp: at stage s the lanes with bit s
+    // clear (rows r) trade their columns c + s (bit s of c set) for the columns
+    // c of rows r + s.  Afterwards lane l's a[g] holds, at bit r, row
+    // k0 + 32 warp + r of column j0 + 32 g + l.
+#pragma unroll
+    for (int sh = 16; sh >= 1; sh >>= 1) {
+        const u32 m = sh == 16 ? 0x0000FFFFu : sh == 8 ? 0x00FF00FFu : sh == 4 ? 0x0F0F0F0Fu : sh == 2 ? 0x33333333u
+                                                                                                     : 0x55555555u;
+        const bool upper = lane & sh;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            const u32 t = __shfl_xor_sync(0xffffffffu, a[g], sh);
+            a[g] = upper ? ((a[g] & ~m) | ((t >> sh) & m)) : ((a[g] & m) | ((t & m) << sh));
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < 8; ++g) U[32 * g + lane][warp] = a[g];
     __syncthreads();
     if (F4) {
         // column j, k slice q (32 values): 16 bytes, value k in nibble k & 1 of byte k / 2
