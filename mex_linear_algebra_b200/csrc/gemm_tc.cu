@@ -237,13 +237,20 @@ constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
 struct PairCtl {
     u64 full[P_STAGES];   // even CTA: both CTAs' bytes of a stage have landed
     u64 empty[P_STAGES];  // both CTAs: the pair's MMAs have read a stage
-    u64 acc;              // both CTAs: the accumulator is complete
+    u64 acc_full;         // both CTAs: the accumulator holds a finished tile
+    u64 acc_empty;        // even CTA: both CTAs' epilogues have read the accumulator
     u64 drain;
     u32 tmem;
     int abort;
 };
+constexpr int P_EPI_WARPS = 4;
 }  // namespace
 
+// Persistent: cluster c computes tiles c, c + clusters, ... (grouped
+// rasterisation over 256 x 256 tiles).  The stage ring runs on across tiles,
+// so the producer fills the next tile's stages while the current tile's last
+// MMAs and its epilogue run; the MMA thread starts a tile once both CTAs'
+// epilogues have read the previous one out of TMEM.
 template <bool F4>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
 gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -258,22 +265,24 @@ gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 rank = ptx::cluster_ctarank();
     const bool leader = rank == 0;
-
-    // grouped rasterisation over 256 x 256 tiles
-    const int t = blockIdx.x >> 1;
-    const int per_group = GROUP_M * tiles_n;
-    const int group = t / per_group;
-    const int first_m = group * GROUP_M;
-    const int gsize = (tiles_m - first_m) < GROUP_M ? (tiles_m - first_m) : GROUP_M;
-    const int tm = first_m + (t % per_group) % gsize;
-    const int tn = (t % per_group) / gsize;
+    const int cid = blockIdx.x >> 1, clusters = gridDim.x >> 1;
+    const int ntiles = tiles_m * tiles_n;
+    auto coords = [&](int t, int &tm, int &tn) {
+        const int per_group = GROUP_M * tiles_n;
+        const int group = t / per_group;
+        const int first_m = group * GROUP_M;
+        const int gsize = (tiles_m - first_m) < GROUP_M ? (tiles_m - first_m) : GROUP_M;
+        tm = first_m + (t % per_group) % gsize;
+        tn = (t % per_group) / gsize;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < P_STAGES; ++s) {
             ptx::mbar_init(&ctl->full[s], 1);
             ptx::mbar_init(&ctl->empty[s], 1);
         }
-        ptx::mbar_init(&ctl->acc, 1);
+        ptx::mbar_init(&ctl->acc_full, 1);
+        ptx::mbar_init(&ctl->acc_empty, 2 * P_EPI_WARPS);
         ptx::mbar_init(&ctl->drain, 1);
         ctl->abort = 0;
         ptx::fence_barrier_init();
@@ -306,48 +315,63 @@ gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     if (warp == 0) {
         if (lane == 0) {
             const u32 full0 = ptx::mapa_shared(ptx::smem_u32(&ctl->full[0]), 0);
-            for (int ks = 0; ks < kstages; ++ks) {
-                const int s = ks % P_STAGES, round = ks / P_STAGES;
-                if (round > 0 && !ptx::mbar_wait(&ctl->empty[s], (round - 1) & 1, err)) {
-                    *abort_flag = 1;
-                    break;
+            int g = 0;  // stage counter over all tiles of this cluster
+            bool ok = true;
+            for (int t = cid; t < ntiles && ok; t += clusters) {
+                int tm, tn;
+                coords(t, tm, tn);
+                for (int ks = 0; ks < kstages; ++ks, ++g) {
+                    const int s = g % P_STAGES, round = g / P_STAGES;
+                    if ((round > 0 && !ptx::mbar_wait(&ctl->empty[s], (round - 1) & 1, err)) || *abort_flag) {
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *sa = smem + s * P_STAGE_BYTES;
+                    if (leader) ptx::mbar_arrive_expect_tx(&ctl->full[s], 2 * P_STAGE_BYTES);
+                    const u32 bar = full0 + (u32)(s * sizeof(u64));
+                    ptx::tma_load_2d_pair(sa, &tmA, bar, ks * BK, tm * 256 + (int)rank * 128);
+                    ptx::tma_load_2d_pair(sa + P_A_BYTES, &tmB, bar, ks * BK, tn * 256 + (int)rank * 128);
                 }
-                if (*abort_flag) break;
-                unsigned char *sa = smem + s * P_STAGE_BYTES;
-                if (leader) ptx::mbar_arrive_expect_tx(&ctl->full[s], 2 * P_STAGE_BYTES);
-                const u32 bar = full0 + (u32)(s * sizeof(u64));
-                ptx::tma_load_2d_pair(sa, &tmA, bar, ks * BK, tm * 256 + (int)rank * 128);
-                ptx::tma_load_2d_pair(sa + P_A_BYTES, &tmB, bar, ks * BK, tn * 256 + (int)rank * 128);
             }
         }
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             constexpr u32 idesc = F4 ? ptx::idesc_mxf4(256, BN) : ptx::idesc_i8(256, BN);
             bool ok = true;
-            for (int ks = 0; ks < kstages; ++ks) {
-                const int s = ks % P_STAGES, round = ks / P_STAGES;
-                if (!ptx::mbar_wait(&ctl->full[s], round & 1, err) || *abort_flag) {
-                    *abort_flag = 1;
+            int g = 0, i = 0;
+            for (int t = cid; t < ntiles && ok; t += clusters, ++i) {
+                // the previous tile has left TMEM (both CTAs)
+                if (i > 0 && (!ptx::mbar_wait_cluster(&ctl->acc_empty, (i - 1) & 1, err) || *abort_flag)) {
                     ok = false;
                     break;
                 }
                 ptx::tc_fence_after();
-                const u32 a0 = ptx::smem_u32(smem + s * P_STAGE_BYTES);
-                const u32 b0 = a0 + P_A_BYTES;
+                for (int ks = 0; ks < kstages; ++ks, ++g) {
+                    const int s = g % P_STAGES, round = g / P_STAGES;
+                    if (!ptx::mbar_wait(&ctl->full[s], round & 1, err) || *abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const u32 a0 = ptx::smem_u32(smem + s * P_STAGE_BYTES);
+                    const u32 b0 = a0 + P_A_BYTES;
 #pragma unroll
-                for (int kk = 0; kk < BK / 32; ++kk) {
-                    if constexpr (F4)
-                        ptx::umma_mxf4_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
-                                            idesc, tmem + SF_COL, tmem + SF_COL + 8, (ks | kk) != 0);
-                    else
-                        ptx::umma_i8_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
-                                          idesc, (ks | kk) != 0);
+                    for (int kk = 0; kk < BK / 32; ++kk) {
+                        if constexpr (F4)
+                            ptx::umma_mxf4_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32),
+                                                ptx::desc_k_sw128(b0 + kk * 32), idesc, tmem + SF_COL,
+                                                tmem + SF_COL + 8, (ks | kk) != 0);
+                        else
+                            ptx::umma_i8_pair(tmem, ptx::desc_k_sw128(a0 + kk * 32), ptx::desc_k_sw128(b0 + kk * 32),
+                                              idesc, (ks | kk) != 0);
+                    }
+                    ptx::umma_commit_pair(&ctl->empty[s], 0x3);
                 }
-                ptx::umma_commit_pair(&ctl->empty[s], 0x3);
+                if (ok) ptx::umma_commit_pair(&ctl->acc_full, 0x3);
             }
-            if (ok) {
-                ptx::umma_commit_pair(&ctl->acc, 0x3);
-            } else {
+            if (!ok) {
+                *abort_flag = 1;
                 // drain the MMAs still reading either CTA's shared memory
                 ptx::umma_commit_pair(&ctl->drain, 0x1);
                 ptx::mbar_wait(&ctl->drain, 0, nullptr);
@@ -355,10 +379,19 @@ gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         }
         __syncwarp();
     } else {
-        const bool ok = ptx::mbar_wait(&ctl->acc, 0, err);
-        ptx::tc_fence_after();
-        if (ok && !*abort_flag) {
-            const int ew = warp & 3;  // TMEM lane quarter this warp may access
+        const int ew = warp & 3;  // TMEM lane quarter this warp may access
+        const u32 acc_empty0 = ptx::mapa_shared(ptx::smem_u32(&ctl->acc_empty), 0);
+        const i64 nw = words_of(n);
+        int i = 0;
+        for (int t = cid; t < ntiles; t += clusters, ++i) {
+            const bool ok = ptx::mbar_wait(&ctl->acc_full, i & 1, err);
+            ptx::tc_fence_after();
+            if (!ok || *abort_flag) {
+                *abort_flag = 1;
+                break;
+            }
+            int tm, tn;
+            coords(t, tm, tn);
             const i64 row = (i64)tm * 256 + (i64)rank * 128 + ew * 32 + lane;
             u32 bits[BN / 32];
 #pragma unroll
@@ -374,7 +407,10 @@ gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 }
                 bits[c] = b;
             }
-            const i64 nw = words_of(n);
+            // this warp's TMEM reads are done: the next tile may overwrite them
+            ptx::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive_cluster(acc_empty0);
             if (row < m) {
 #pragma unroll
                 for (int q = 0; q < BN / 64; ++q) {
@@ -382,8 +418,6 @@ gemm_tc_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     if (w < nw) C[row * ldc + w] = (u64)bits[2 * q] | ((u64)bits[2 * q + 1] << 32);
                 }
             }
-        } else {
-            *abort_flag = 1;
         }
     }
 
@@ -476,7 +510,8 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
         if (st != MELA_OK) return st;
         st = make_map(&mb, Bt8, np, kp, 128);
         if (st != MELA_OK) return st;
-        const unsigned grid = (unsigned)(2 * (mp / 256) * tiles_n);
+        const i64 ntiles = (mp / 256) * tiles_n, clusters_max = sm_count() / 2;
+        const unsigned grid = (unsigned)(2 * (ntiles < clusters_max ? ntiles : clusters_max));
         if (fp4) {
             MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_tc_pair_kernel<true>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));

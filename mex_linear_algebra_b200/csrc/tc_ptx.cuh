@@ -178,6 +178,39 @@ __device__ __forceinline__ u32 mapa_shared(u32 addr, u32 rank)
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
     return r;
 }
+// Arrive (release at cluster scope) on an mbarrier given by its
+// shared::cluster address, possibly in the other CTA of the pair.
+__device__ __forceinline__ void mbar_arrive_cluster(u32 bar_cluster)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+// Bounded wait (acquire at cluster scope) for a phase of a barrier of this
+// CTA that the other CTA of the pair arrives on.
+__device__ __forceinline__ bool mbar_try_wait_cluster(u64 *bar, u32 parity)
+{
+    u32 ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(u64 *bar, u32 parity, u32 *err)
+{
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait_cluster(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitLimitNs) {
+            if (err) atomicOr(err, kErrWaitTimeout);
+            return false;
+        }
+    }
+}
 // Every thread of both CTAs arrives; returns once all have.
 __device__ __forceinline__ void cluster_sync()
 {
