@@ -554,7 +554,7 @@ def run_mela(args, ws, rank, local):
                          "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                          # dram read + write bytes of one launch: an ncu capture of the FP4 kernel at
                          # 16384^3 (0.715 GB) scaled by m*n*k to the full launch
-                         "traffic": (0.7154e9 * (M * N * K) / 16384 ** 3) if args.variant == "tc_fp4" else None,
+                         "traffic": (0.8050e9 * (M * N * K) / 16384 ** 3) if args.variant == "tc_fp4" else None,
                          "traffic_unit": "bytes per launch",
                          "kernel": "gemm_tc_pair_kernel", "kernel_ms": round(kern_avg, 4),
                          "peak_source": ("2 x dense INT8 measured in this run (cuBLASLt int8 GEMM 8192^3 "
