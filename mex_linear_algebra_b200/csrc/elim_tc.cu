@@ -565,7 +565,7 @@ constexpr int U_STAGES = 4;                   // X8 tiles in flight
 constexpr int U_BSTAGES = 1;                  // Rt8 strips in shared memory
 constexpr int U_STAGE_BYTES = 2 * 2 * UM * 4 * 8;  // per accumulator, two 128-row x 4-word stages
 constexpr int U_SMEM = U_BSTAGES * UB_BYTES + U_STAGES * UA_BYTES + U_STAGE_BYTES + 1024 + 256;
-constexpr int U_MCH = 8;                      // row tiles per work unit
+constexpr int U_MCH = 8;                      // row tiles per work unit (far part)
 constexpr int U_EPI_THREADS = 256;           // warps draining one accumulator: 2 per TMEM lane quarter
 constexpr int U_THREADS = 64 + 2 * U_EPI_THREADS;  // and the same for the other accumulator
 
@@ -591,17 +591,22 @@ struct UCtl {
 __global__ void __launch_bounds__(U_THREADS, 1)
 tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmR,
                  u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const WinState *ws, const int *__restrict__ ulist,
-                 unsigned char *live, int strip_lo, int strip_hi, u32 *err)
+                 unsigned char *live, int strip_lo, int strip_hi, int skip, int mch, u32 *err)
 {
-    // strips strip_lo .. strip_hi-1 (256 columns each, from the window's first column)
+    // strips strip_lo .. strip_hi-1 (256 columns each, from the window's first
+    // column) except strip `skip` (-1: none); work units of mch row tiles
     const int rt = ws->rt, nu = ws->nu;
     if (rt == 0 || nu == 0) return;
     const i64 lw = wc - w;
     const int s_end = (int)((lw + 3) / 4) < strip_hi ? (int)((lw + 3) / 4) : strip_hi;
-    const int strips = s_end - strip_lo;
+    const int strips = s_end - strip_lo - (skip >= strip_lo && skip < s_end ? 1 : 0);
     if (strips <= 0) return;
+    auto strip_of = [&](long long vs) -> int {
+        const int st = strip_lo + (int)vs;
+        return (skip >= 0 && st >= skip) ? st + 1 : st;
+    };
     const int mt = (nu + UM - 1) / UM;
-    const int chunks = (mt + U_MCH - 1) / U_MCH;
+    const int chunks = (mt + mch - 1) / mch;
     const long long units = (long long)strips * chunks;
     const long long ub = units * blockIdx.x / gridDim.x, ue = units * (blockIdx.x + 1) / gridDim.x;
     if (ub >= ue) return;
@@ -657,7 +662,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             for (int q = 0; q < U_BSTAGES; ++q) last_b[q] = -1;
             bool ok = true;
             for (long long u = ub; u < ue && ok; ++u) {
-                const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
+                const int strip = strip_of(u / chunks), chunk = (int)(u % chunks);
                 if (strip != prev_strip) {
                     const int bs = nbl % U_BSTAGES;
                     if (nbl >= U_BSTAGES && !ptx::mbar_wait(&ctl->bempty[bs], ((nbl / U_BSTAGES) - 1) & 1, err)) {
@@ -676,8 +681,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
                     ++nbl;
                     prev_strip = strip;
                 }
-                const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
-                for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+                const int t1 = (chunk + 1) * mch < mt ? (chunk + 1) * mch : mt;
+                for (int tile = chunk * mch; tile < t1; ++tile, ++it) {
                     const int s = it % U_STAGES;
                     if (it >= U_STAGES && !ptx::mbar_wait(&ctl->aempty[s], ((it / U_STAGES) - 1) & 1, err)) {
                         ok = false;
@@ -709,7 +714,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             int nbl = 0, it = 0, prev_strip = -1, bs = 0;
             bool ok = true;
             for (long long u = ub; u < ue && ok; ++u) {
-                const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
+                const int strip = strip_of(u / chunks), chunk = (int)(u % chunks);
                 if (strip != prev_strip) {
                     bs = nbl % U_BSTAGES;
                     if (!ptx::mbar_wait(&ctl->bfull[bs], (nbl / U_BSTAGES) & 1, err) || *abort_flag) {
@@ -720,8 +725,8 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
                     prev_strip = strip;
                 }
                 const u32 b0 = ptx::smem_u32(sB + bs * UB_BYTES);
-                const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
-                for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+                const int t1 = (chunk + 1) * mch < mt ? (chunk + 1) * mch : mt;
+                for (int tile = chunk * mch; tile < t1; ++tile, ++it) {
                     const int s = it % U_STAGES, acc = it & 1;
                     if (!ptx::mbar_wait(&ctl->afull[s], (it / U_STAGES) & 1, err) ||
                         (it >= 2 && !ptx::mbar_wait(&ctl->accempty[acc], ((it >> 1) - 1) & 1, err)) ||
@@ -743,7 +748,7 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
                 }
                 if (!ok) break;
                 // the strip's buffer is free once this unit's products are done
-                const bool next_same = (u + 1 < ue) && (strip_lo + (int)((u + 1) / chunks) == strip);
+                const bool next_same = (u + 1 < ue) && (strip_of((u + 1) / chunks) == strip);
                 if (!next_same) ptx::umma_commit(&ctl->bempty[bs]);
             }
             if (!ok) {
@@ -825,11 +830,11 @@ tc_update_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
             return good;
         };
         for (long long u = ub; u < ue; ++u) {
-            const int strip = strip_lo + (int)(u / chunks), chunk = (int)(u % chunks);
+            const int strip = strip_of(u / chunks), chunk = (int)(u % chunks);
             const i64 w0 = w + (i64)strip * 4;
             const int nw = (wc - w0) < 4 ? (int)(wc - w0) : 4;
-            const int t1 = (chunk + 1) * U_MCH < mt ? (chunk + 1) * U_MCH : mt;
-            for (int tile = chunk * U_MCH; tile < t1; ++tile, ++it) {
+            const int t1 = (chunk + 1) * mch < mt ? (chunk + 1) * mch : mt;
+            for (int tile = chunk * mch; tile < t1; ++tile, ++it) {
                 if ((it & 1) != g) continue;
                 // fetch this tile's words (coalesced layout), then finish the previous tile
                 int row[2] = {-1, -1};
@@ -963,13 +968,13 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     const int sms = sm_count();
     const i64 coef_blocks_full = (m + 255) / 256;
     const int coef_blocks = (int)(coef_blocks_full < (i64)sms * 8 ? coef_blocks_full : (i64)sms * 8);
-    const i64 chunks_max = (L.mpad / UM + U_MCH - 1) / U_MCH;
+    const i64 tiles_max = L.mpad / UM, chunks_max = (tiles_max + U_MCH - 1) / U_MCH;
     u32 *err = device_error_word();
 
-    // Look-ahead: the update of window w is split into its first two strips
-    // (window w itself and window w+1), run on the caller's stream before
-    // window w+1 is factored, and the rest, forked to the side stream so that
-    // it runs while window w+1 is factored (on an SM the fork leaves free).
+    // Look-ahead: the update of window w is split into its second strip
+    // (window w+1's columns), run on the caller's stream before window w+1 is
+    // factored, and the rest, forked to the side stream so that it runs while
+    // window w+1 is factored (on an SM the fork leaves free).
     // Window w+1's combine waits for it: it reads the pivot rows' later words,
     // and its coefficient and R buffers are the ones the rest still reads.
     // Window states and row flags alternate by window parity so that the
@@ -999,18 +1004,27 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
             window_coef_kernel<<<coef_blocks, 256, 0, s>>>(M, ld, m, wc, w, list, stamp, wid, rref, cur, ulist, X8,
                                                            live);
             window_rt_kernel<<<(unsigned)lw, 256, 0, s>>>(M, ld, w, Rbuf, wc, cur, Rt8);
+            // near: strip 1 (the next window's columns, all the next
+            // factorization reads), one row tile per CTA; far: strip 0 (the
+            // window's own columns: only the RREF needs them -- for the rank
+            // every updated row is in the window basis' span and its window
+            // part becomes zero) and strips 2.., on the side stream
             const i64 strips = (lw + 3) / 4;
-            const i64 near = strips < 2 ? strips : 2;
-            const int grid_near = (int)(near * chunks_max < sms ? near * chunks_max : sms);
-            tc_update_kernel<<<grid_near, U_THREADS, U_SMEM, s>>>(mx, mr, M, ld, wc, w, cur, ulist, live, 0, 2, err);
-            if (strips > 2) {
-                const i64 units = (strips - 2) * chunks_max;
+            if (strips >= 2) {
+                const int grid_near = (int)(tiles_max < sms ? tiles_max : sms);
+                tc_update_kernel<<<grid_near, U_THREADS, U_SMEM, s>>>(mx, mr, M, ld, wc, w, cur, ulist, live, 1, 2,
+                                                                      -1, 1, err);
+            }
+            const int far_lo = rref ? 0 : 2, far_skip = (rref && strips >= 2) ? 1 : -1;
+            const i64 far_strips = (strips > far_lo ? strips - far_lo : 0) - (far_skip >= 0 ? 1 : 0);
+            if (far_strips > 0) {
+                const i64 units = far_strips * chunks_max;
                 const int cap = sms > 4 ? sms - 2 : sms;  // SMs left for the next factorization
                 const int grid_far = (int)(units < cap ? units : cap);
                 MELA_CUDA_TRY(cudaEventRecord(ev_fork, s));
                 MELA_CUDA_TRY(cudaStreamWaitEvent(s2, ev_fork, 0));
-                tc_update_kernel<<<grid_far, U_THREADS, U_SMEM, s2>>>(mx, mr, M, ld, wc, w, cur, ulist, live, 2,
-                                                                     (int)strips, err);
+                tc_update_kernel<<<grid_far, U_THREADS, U_SMEM, s2>>>(mx, mr, M, ld, wc, w, cur, ulist, live, far_lo,
+                                                                     (int)strips, far_skip, U_MCH, err);
                 MELA_CUDA_TRY(cudaEventRecord(ev_join, s2));
                 forked = true;
             }
