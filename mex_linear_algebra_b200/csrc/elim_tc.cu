@@ -104,10 +104,6 @@ __device__ __forceinline__ void xor4s(u64 (&a)[WW], const u64 *b)
 }
 __device__ __forceinline__ bool any4(const u64 (&v)[WW]) { return (v[0] | v[1] | v[2] | v[3]) != 0; }
 
-__device__ __forceinline__ int lead4(const u64 (&v)[WW])
-{
-    return v[0] ? ctz64w(v[0]) : (v[1] ? 64 + ctz64w(v[1]) : (v[2] ? 128 + ctz64w(v[2]) : 192 + ctz64w(v[3])));
-}
 
 // Exclusive position of this thread's flag among the block's flags (thread
 // order) and the block total; every thread of the block must call it.
@@ -200,14 +196,18 @@ window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int
                 }
             }
         }
-        // Gauss-Jordan among the chunk's residual rows, a pivot per barrier.
-        // A row's key is (leading bit, slot); the next pivot is the smallest
-        // key.  Only the row holding its warp's smallest key publishes itself
-        // to shared memory, its tag already carrying the P-index it would
-        // enter as, so the pivot is always published.
+        // Gauss-Jordan among the chunk's residual rows, a pivot per barrier,
+        // one 64-column word of the window at a time.  A row's key is
+        // (leading bit, slot); the next pivot is the smallest key.  Inside
+        // word q every unused row is zero in the words before q, so its key
+        // comes from word q alone and a pivot row is XORed in from word q on;
+        // word q is done once no unused row has a bit left there.  Only the
+        // row holding its warp's smallest key publishes itself to shared
+        // memory, its tag already carrying the P-index it would enter as, so
+        // the pivot is always published.
         bool used = false;
         int myj = -1;
-        unsigned key = any4(cx) ? ((unsigned)lead4(cx) << 10 | (unsigned)tid) : NOKEY;
+        unsigned key = NOKEY;
         auto publish = [&](unsigned *kslot, int jn) {
             const unsigned mk = __reduce_min_sync(0xffffffffu, key);
             if (key == mk && key != NOKEY) {
@@ -222,42 +222,47 @@ window_factor_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 n, i64 w, int
             }
             if (lane == 0 && mk != NOKEY) atomicMin(kslot, mk);
         };
-        if (tid < 3) S.keys[tid] = NOKEY;
-        __syncthreads();
-        publish(&S.keys[0], nb0);
-        __syncthreads();
-        int nnew = 0, kr = 0;  // kr: slot holding this iteration's key
-        for (;;) {
-            const unsigned kk = S.keys[kr];
-            if (kk == NOKEY || nb0 + nnew >= valid) break;
-            const int kn = kr == 2 ? 0 : kr + 1, kz = kn == 2 ? 0 : kn + 1;
-            if (tid == 0) S.keys[kz] = NOKEY;  // read last in the previous iteration
-            const int p = (int)(kk & 1023u), L = (int)(kk >> 10);
-            if (tid == p) {
-                used = true;
-                myj = nb0 + nnew;
-                key = NOKEY;
-                S.newslot[nnew] = p;
-                S.newlead[nnew] = L;
-                S.prow[myj] = row;
-            } else if (bit_of(cx, L)) {
-                const ulonglong2 *pv = reinterpret_cast<const ulonglong2 *>(S.cx[p]);
-                const ulonglong2 *pt = reinterpret_cast<const ulonglong2 *>(S.ct[p]);
-                const ulonglong2 v0 = pv[0], v1 = pv[1], t0 = pt[0], t1 = pt[1];
-                cx[0] ^= v0.x;
-                cx[1] ^= v0.y;
-                cx[2] ^= v1.x;
-                cx[3] ^= v1.y;
-                ct[0] ^= t0.x;
-                ct[1] ^= t0.y;
-                ct[2] ^= t1.x;
-                ct[3] ^= t1.y;
-                if (!used) key = any4(cx) ? ((unsigned)lead4(cx) << 10 | (unsigned)tid) : NOKEY;
-            }
-            ++nnew;
-            publish(&S.keys[kn], nb0 + nnew);
-            kr = kn;
+        int nnew = 0;
+#pragma unroll
+        for (int q = 0; q < WW; ++q) {
+            if (nb0 + nnew >= valid) break;  // uniform
+            key = (!used && cx[q]) ? ((unsigned)(64 * q + ctz64w(cx[q])) << 10 | (unsigned)tid) : NOKEY;
+            __syncthreads();  // the previous word's last keys have been read
+            if (tid < 3) S.keys[tid] = NOKEY;
             __syncthreads();
+            publish(&S.keys[0], nb0 + nnew);
+            __syncthreads();
+            int kr = 0;  // slot holding this iteration's key
+            for (;;) {
+                const unsigned kk = S.keys[kr];
+                if (kk == NOKEY || nb0 + nnew >= valid) break;
+                const int kn = kr == 2 ? 0 : kr + 1, kz = kn == 2 ? 0 : kn + 1;
+                if (tid == 0) S.keys[kz] = NOKEY;  // read last in the previous iteration
+                const int p = (int)(kk & 1023u), L = (int)(kk >> 10);
+                if (tid == p) {
+                    used = true;
+                    myj = nb0 + nnew;
+                    key = NOKEY;
+                    S.newslot[nnew] = p;
+                    S.newlead[nnew] = L;
+                    S.prow[myj] = row;
+                } else if ((cx[q] >> (L & 63)) & 1) {
+                    const u64 *pv = S.cx[p];
+                    const ulonglong2 *pt = reinterpret_cast<const ulonglong2 *>(S.ct[p]);
+                    const ulonglong2 t0 = pt[0], t1 = pt[1];
+#pragma unroll
+                    for (int qq = q; qq < WW; ++qq) cx[qq] ^= pv[qq];
+                    ct[0] ^= t0.x;
+                    ct[1] ^= t0.y;
+                    ct[2] ^= t1.x;
+                    ct[3] ^= t1.y;
+                    if (!used) key = cx[q] ? ((unsigned)(64 * q + ctz64w(cx[q])) << 10 | (unsigned)tid) : NOKEY;
+                }
+                ++nnew;
+                publish(&S.keys[kn], nb0 + nnew);
+                kr = kn;
+                __syncthreads();
+            }
         }
         __syncthreads();  // every key is read before the next chunk publishes
         if (nnew == 0) continue;  // uniform
