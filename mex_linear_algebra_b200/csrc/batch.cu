@@ -237,8 +237,13 @@ __host__ __device__ inline long long big_scratch_words(long long m, long long n)
 namespace {
 constexpr int kBigWarps = kThreads / 32;
 constexpr int kTW = 32;  // words per update chunk (one per lane)
+constexpr int kRegThreads = 128;  // threads holding a panel in registers (m <= 1024)
+constexpr int kRegRows = 8;        // rows per thread there
+constexpr int kRegBar = 6;         // their named barrier
 struct BigSmem {
     u64 coef[64];
+    u64 pub[2][4][2];      // per warp: its candidate pivot's panel word and tag (by bit parity)
+    alignas(16) unsigned wmin[2][4];  // per warp: its candidate pivot row
     int bits[64], srow[64];
     int slots[4];
     u64 T[16][16][kTW];  // nibble tables of the current chunk
@@ -250,6 +255,15 @@ struct BigSmem {
 constexpr size_t kBigExtra = (size_t)kSmemTotal - ((sizeof(BigSmem) + 15) & ~(size_t)15);
 static_assert(sizeof(BigSmem) <= (size_t)kSmemTotal, "big-matrix shared memory");
 }  // namespace
+
+// Element i (0..7, per thread) of a register array, by a select tree.
+__device__ __forceinline__ u64 sel8(const u64 (&v)[8], int i)
+{
+    const u64 a0 = (i & 1) ? v[1] : v[0], a1 = (i & 1) ? v[3] : v[2], a2 = (i & 1) ? v[5] : v[4],
+              a3 = (i & 1) ? v[7] : v[6];
+    const u64 b0 = (i & 2) ? a1 : a0, b1 = (i & 2) ? a3 : a2;
+    return (i & 4) ? b1 : b0;
+}
 
 // 32x32 bit transposes by warp ballots over a CTA: dst (cols x rows bits,
 // 32-bit words, pitch dld) = src^T, where src row r, 32-bit word x is
@@ -329,57 +343,131 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
 
     int r = 0;
     for (int w = 0; w < wc && r < m; ++w) {
-        // 1. panel words, pivot search for bit 0
-        if (tid < 3) S.slots[tid] = INT_MAX;
-        __syncthreads();
-        unsigned best = INT_MAX;
-        for (int j = tid; j < m; j += kThreads) {
-            const u64 word = A[(size_t)j * wc + w];
-            ysnap[j] = word;
-            const u64 y = active[j] == 1 ? word : 0ull;
-            yv[j] = y;
-            tag[j] = 0;
-            if ((y & 1ull) && best == (unsigned)INT_MAX) best = j;
-        }
-        best = __reduce_min_sync(0xffffffffu, best);
-        if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[0], (int)best);
-        __syncthreads();
-        // 2. per-bit elimination of the panel words with combination tags
         int k = 0;
         u64 pmask = 0;
-        for (int b = 0; b < 64; ++b) {
-            const int p = S.slots[b % 3];
-            if (tid == 0) S.slots[(b + 2) % 3] = INT_MAX;
-            if (p != INT_MAX) {
-                const u64 yp = yv[p], tp = tag[p] ^ (1ull << k);
+        if (m <= kRegRows * kRegThreads) {
+            // 1-2. the panel in registers of the first four warps: thread l
+            // holds rows l + 128 i.  Per bit one named barrier: each warp
+            // publishes its lowest unused row holding the bit (index, panel
+            // word and tag); the lowest of the four is the pivot.
+            for (int j = tid; j < m; j += kThreads) ysnap[j] = A[(size_t)j * wc + w];
+            __syncthreads();
+            if (tid < kRegThreads) {
+                const int warp = tid >> 5;
+                u64 y[kRegRows], t[kRegRows];
+                u32 unused = 0;
+#pragma unroll
+                for (int i = 0; i < kRegRows; ++i) {
+                    const int j = tid + kRegThreads * i;
+                    const int a = j < m ? active[j] : 0;
+                    y[i] = a == 1 ? ysnap[j] : 0ull;
+                    t[i] = 0;
+                    unused |= (a == 1 ? 1u : 0u) << i;
+                }
+                for (int b = 0; b < 64; ++b) {
+                    u32 cm = 0;
+#pragma unroll
+                    for (int i = 0; i < kRegRows; ++i) cm |= (u32)((y[i] >> b) & 1ull) << i;
+                    cm &= unused;
+                    const int ib = __ffs((int)cm) - 1;
+                    const unsigned jb = ib >= 0 ? (unsigned)(tid + kRegThreads * ib) : (unsigned)INT_MAX;
+                    const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
+                    const int par = b & 1;
+                    if (jb == wm && wm != (unsigned)INT_MAX) {
+                        S.pub[par][warp][0] = sel8(y, ib);
+                        S.pub[par][warp][1] = sel8(t, ib);
+                    }
+                    if (lane == 0) S.wmin[par][warp] = wm;
+                    asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
+                    const uint4 wmv = *reinterpret_cast<const uint4 *>(S.wmin[par]);
+                    const unsigned pm = min(min(wmv.x, wmv.y), min(wmv.z, wmv.w));
+                    if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
+                    const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
+                    const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
+                    if (tid == 0) {
+                        S.bits[k] = b;
+                        S.srow[k] = pr;
+                    }
+                    const u64 bit = 1ull << b;
+#pragma unroll
+                    for (int i = 0; i < kRegRows; ++i) {
+                        const int j = tid + kRegThreads * i;
+                        if (j == pr) {
+                            unused &= ~(1u << i);
+                        } else if (y[i] & bit) {
+                            y[i] ^= yp;
+                            t[i] ^= tp;
+                        }
+                    }
+                    pmask |= bit;
+                    ++k;
+                }
+#pragma unroll
+                for (int i = 0; i < kRegRows; ++i) {
+                    const int j = tid + kRegThreads * i;
+                    if (j < m) tag[j] = t[i];
+                }
                 if (tid == 0) {
-                    S.bits[k] = b;
-                    S.srow[k] = p;
+                    S.p = k;
+                    S.pm = pmask;
                 }
-                if (p % kThreads == tid) active[p] = 2;
-                const u64 bit = 1ull << b;
-                for (int j = tid; j < m; j += kThreads) {
-                    if (j == p || active[j] == 0) continue;
-                    if (yv[j] & bit) {
-                        yv[j] ^= yp;
-                        tag[j] ^= tp;
-                    }
-                }
-                pmask |= bit;
-                ++k;
-            }
-            if (b < 63) {
-                const u64 bit = 1ull << (b + 1);
-                best = INT_MAX;
-                for (int j = tid; j < m; j += kThreads)
-                    if (active[j] == 1 && (yv[j] & bit)) {
-                        best = j;
-                        break;
-                    }
-                best = __reduce_min_sync(0xffffffffu, best);
-                if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[(b + 1) % 3], (int)best);
             }
             __syncthreads();
+            k = S.p;
+            pmask = S.pm;
+            for (int q = tid; q < k; q += kThreads) active[S.srow[q]] = 2;
+            __syncthreads();
+        } else {
+            // 1. panel words, pivot search for bit 0
+            if (tid < 3) S.slots[tid] = INT_MAX;
+            __syncthreads();
+            unsigned best = INT_MAX;
+            for (int j = tid; j < m; j += kThreads) {
+                const u64 word = A[(size_t)j * wc + w];
+                ysnap[j] = word;
+                const u64 y = active[j] == 1 ? word : 0ull;
+                yv[j] = y;
+                tag[j] = 0;
+                if ((y & 1ull) && best == (unsigned)INT_MAX) best = j;
+            }
+            best = __reduce_min_sync(0xffffffffu, best);
+            if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[0], (int)best);
+            __syncthreads();
+            // 2. per-bit elimination of the panel words with combination tags
+            for (int b = 0; b < 64; ++b) {
+                const int p = S.slots[b % 3];
+                if (tid == 0) S.slots[(b + 2) % 3] = INT_MAX;
+                if (p != INT_MAX) {
+                    const u64 yp = yv[p], tp = tag[p] ^ (1ull << k);
+                    if (tid == 0) {
+                        S.bits[k] = b;
+                        S.srow[k] = p;
+                    }
+                    if (p % kThreads == tid) active[p] = 2;
+                    const u64 bit = 1ull << b;
+                    for (int j = tid; j < m; j += kThreads) {
+                        if (j == p || active[j] == 0) continue;
+                        if (yv[j] & bit) {
+                            yv[j] ^= yp;
+                            tag[j] ^= tp;
+                        }
+                    }
+                    pmask |= bit;
+                    ++k;
+                }
+                if (b < 63) {
+                    const u64 bit = 1ull << (b + 1);
+                    best = INT_MAX;
+                    for (int j = tid; j < m; j += kThreads)
+                        if (active[j] == 1 && (yv[j] & bit)) {
+                            best = j;
+                            break;
+                        }
+                    best = __reduce_min_sync(0xffffffffu, best);
+                    if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[(b + 1) % 3], (int)best);
+                }
+                __syncthreads();
+            }
         }
         const int p = k;
         if (p == 0) continue;
