@@ -364,43 +364,45 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                     t[i] = 0;
                     unused |= (a == 1 ? 1u : 0u) << i;
                 }
-                for (int b = 0; b < 64; ++b) {
-                    u32 cm = 0;
 #pragma unroll
-                    for (int i = 0; i < kRegRows; ++i) cm |= (u32)((y[i] >> b) & 1ull) << i;
-                    cm &= unused;
-                    const int ib = __ffs((int)cm) - 1;
-                    const unsigned jb = ib >= 0 ? (unsigned)(tid + kRegThreads * ib) : (unsigned)INT_MAX;
-                    const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
-                    const int par = b & 1;
-                    if (jb == wm && wm != (unsigned)INT_MAX) {
-                        S.pub[par][warp][0] = sel8(y, ib);
-                        S.pub[par][warp][1] = sel8(t, ib);
-                    }
-                    if (lane == 0) S.wmin[par][warp] = wm;
-                    asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
-                    const uint4 wmv = *reinterpret_cast<const uint4 *>(S.wmin[par]);
-                    const unsigned pm = min(min(wmv.x, wmv.y), min(wmv.z, wmv.w));
-                    if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
-                    const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
-                    const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
-                    if (tid == 0) {
-                        S.bits[k] = b;
-                        S.srow[k] = pr;
-                    }
-                    const u64 bit = 1ull << b;
+                for (int half = 0; half < 2; ++half) {
+                    for (int bb = 0; bb < 32; ++bb) {
+                        const int b = 32 * half + bb;
+                        u32 cm = 0;
 #pragma unroll
-                    for (int i = 0; i < kRegRows; ++i) {
-                        const int j = tid + kRegThreads * i;
-                        if (j == pr) {
-                            unused &= ~(1u << i);
-                        } else if (y[i] & bit) {
-                            y[i] ^= yp;
-                            t[i] ^= tp;
+                        for (int i = 0; i < kRegRows; ++i) cm |= (((u32)(y[i] >> (32 * half)) >> bb) & 1u) << i;
+                        cm &= unused;
+                        const int ib = __ffs((int)cm) - 1;
+                        const unsigned jb = ib >= 0 ? (unsigned)(tid + kRegThreads * ib) : (unsigned)INT_MAX;
+                        const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
+                        const int par = bb & 1;
+                        if (jb == wm && wm != (unsigned)INT_MAX) {
+                            S.pub[par][warp][0] = sel8(y, ib);
+                            S.pub[par][warp][1] = sel8(t, ib);
                         }
+                        if (lane == 0) S.wmin[par][warp] = wm;
+                        asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
+                        const uint4 wmv = *reinterpret_cast<const uint4 *>(S.wmin[par]);
+                        const unsigned pm = min(min(wmv.x, wmv.y), min(wmv.z, wmv.w));
+                        if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
+                        const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
+                        const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
+                        if (tid == 0) {
+                            S.bits[k] = b;
+                            S.srow[k] = pr;
+                        }
+                        // every other row holding bit b takes the pivot row (branch-free)
+                        const int own = (pr & (kRegThreads - 1)) == tid ? pr / kRegThreads : -1;
+#pragma unroll
+                        for (int i = 0; i < kRegRows; ++i) {
+                            const u64 hit = i == own ? 0ull : 0ull - (u64)(((u32)(y[i] >> (32 * half)) >> bb) & 1u);
+                            y[i] ^= yp & hit;
+                            t[i] ^= tp & hit;
+                        }
+                        if (own >= 0) unused &= ~(1u << own);
+                        pmask |= 1ull << b;
+                        ++k;
                     }
-                    pmask |= bit;
-                    ++k;
                 }
 #pragma unroll
                 for (int i = 0; i < kRegRows; ++i) {
