@@ -265,7 +265,7 @@ __device__ __forceinline__ u64 sel8(const u64 (&v)[8], int i)
     return (i & 4) ? b1 : b0;
 }
 
-// 32x32 bit transposes by warp ballots over a CTA: dst (cols x rows bits,
+// 32x32 bit transposes by warp shuffles over a CTA: dst (cols x rows bits,
 // 32-bit words, pitch dld) = src^T, where src row r, 32-bit word x is
 // srcw(r, x) (rows x cols bits).
 template <typename F>
@@ -276,13 +276,8 @@ __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dl
     for (long long t = warp; t < (long long)rt * ct; t += kBigWarps) {
         const int tr = (int)(t / ct), tc = (int)(t - (long long)tr * ct);
         const int r = tr * 32 + lane;
-        const u32 x = r < rows ? srcw(r, tc) : 0u;
-        u32 keep = 0;
-#pragma unroll
-        for (int b = 0; b < 32; ++b) {
-            const u32 v = __ballot_sync(0xffffffffu, (x >> b) & 1u);
-            if (lane == b) keep = v;
-        }
+        // lane l gets column tc*32 + l, bit b = row tr*32 + b
+        const u32 keep = transpose32_warp(r < rows ? srcw(r, tc) : 0u);
         const int c = tc * 32 + lane;
         if (c < cols) dst[(long long)c * dld + tr] = keep;
     }
@@ -301,7 +296,7 @@ __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dl
 //    a warp per row so that global accesses are contiguous;
 //  * null basis: Zt = (Y)^T with Y row c = (R restricted to free columns)^T
 //    row p when c is pivot column p, the unit vector of its free index
-//    otherwise -- three 32x32 ballot transposes, no per-bit gathers.
+//    otherwise -- three 32x32 shuffle transposes, no per-bit gathers.
 __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restrict__ in,
                                     u64 *__restrict__ zt, long long *ranks, int item,
                                     unsigned char *smem_raw, u64 *g, const FusedOut *fo = nullptr)

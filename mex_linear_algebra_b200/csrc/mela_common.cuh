@@ -59,4 +59,21 @@ __device__ __forceinline__ unsigned long long global_ns()
 // ---------------------------------------------------------------- launch sizing
 int sm_count();  // multiprocessors of the current device (cached per device)
 
+// 32 x 32 bit transpose across a warp: lane r passes row r (bit c = column
+// c); lane c gets column c (bit r = row r).  Five rounds of shuffle
+// butterflies: at round s the lanes with bit s clear trade their columns
+// c + s (bit s of c set) for the columns c of lane r + s.
+__device__ __forceinline__ unsigned transpose32_warp(unsigned v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int sh = 16; sh >= 1; sh >>= 1) {
+        const unsigned m = sh == 16 ? 0x0000FFFFu : sh == 8 ? 0x00FF00FFu : sh == 4 ? 0x0F0F0F0Fu
+                         : sh == 2  ? 0x33333333u : 0x55555555u;
+        const unsigned o = __shfl_xor_sync(0xffffffffu, v, sh);
+        v = (lane & sh) ? ((v & ~m) | ((o >> sh) & m)) : ((v & m) | ((o & m) << sh));
+    }
+    return v;
+}
+
 }  // namespace mela

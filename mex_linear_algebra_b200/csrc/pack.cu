@@ -126,8 +126,9 @@ __global__ void __launch_bounds__(256) unpack_kernel(const u64 *__restrict__ in,
 
 // ---------------------------------------------------------------- transpose
 // Block: 256 input rows x 64 input columns.  Warp w loads rows
-// 32w..32w+31 (one word each); 64 ballots give, per input column b, the 32
-// bits of rows 32w..32w+31.  Output row (column b) receives 4 words.
+// 32w..32w+31 (one word each); two 32x32 warp transposes give, per input
+// column b, the 32 bits of rows 32w..32w+31.  Output row (column b) receives
+// 4 words.
 __global__ void __launch_bounds__(256) transpose_kernel(const u64 *__restrict__ in, i64 ld_in,
                                                         i64 rows, i64 cols,
                                                         u64 *__restrict__ out, i64 ld_out)
@@ -138,17 +139,7 @@ __global__ void __launch_bounds__(256) transpose_kernel(const u64 *__restrict__ 
     const i64 r0 = (i64)blockIdx.y * 256;  // input row group
     const i64 row = r0 + warp * 32 + lane;
     u64 x = (row < rows) ? in[row * ld_in + wcol] : 0ull;
-    u32 keep0 = 0, keep1 = 0;
-#pragma unroll
-    for (int b = 0; b < 32; ++b) {
-        u32 v = __ballot_sync(0xffffffffu, (u32)(x >> b) & 1u);
-        if (lane == b) keep0 = v;
-    }
-#pragma unroll
-    for (int b = 0; b < 32; ++b) {
-        u32 v = __ballot_sync(0xffffffffu, (u32)(x >> (b + 32)) & 1u);
-        if (lane == b) keep1 = v;
-    }
+    const u32 keep0 = transpose32_warp((u32)x), keep1 = transpose32_warp((u32)(x >> 32));
     part[warp][lane] = keep0;
     part[warp][lane + 32] = keep1;
     __syncthreads();
@@ -250,21 +241,10 @@ __global__ void __launch_bounds__(256) expand_t_kernel(const u64 *__restrict__ i
         }
         a[g] = v;
     }
-    // 32 x 32 bit transposes across the warp: at stage s the lanes with bit s
-    // clear (rows r) trade their columns c + s (bit s of c set) for the columns
-    // c of rows r + s.  Afterwards lane l's a[g] holds, at bit r, row
-    // k0 + 32 warp + r of column j0 + 32 g + l.
+    // 32 x 32 bit transposes across the warp: afterwards lane l's a[g] holds,
+    // at bit r, row k0 + 32 warp + r of column j0 + 32 g + l
 #pragma unroll
-    for (int sh = 16; sh >= 1; sh >>= 1) {
-        const u32 m = sh == 16 ? 0x0000FFFFu : sh == 8 ? 0x00FF00FFu : sh == 4 ? 0x0F0F0F0Fu : sh == 2 ? 0x33333333u
-                                                                                                     : 0x55555555u;
-        const bool upper = lane & sh;
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-            const u32 t = __shfl_xor_sync(0xffffffffu, a[g], sh);
-            a[g] = upper ? ((a[g] & ~m) | ((t >> sh) & m)) : ((a[g] & m) | ((t & m) << sh));
-        }
-    }
+    for (int g = 0; g < 8; ++g) a[g] = transpose32_warp(a[g]);
 #pragma unroll
     for (int g = 0; g < 8; ++g) U[32 * g + lane][warp] = a[g];
     __syncthreads();
