@@ -237,13 +237,15 @@ __host__ __device__ inline long long big_scratch_words(long long m, long long n)
 namespace {
 constexpr int kBigWarps = kThreads / 32;
 constexpr int kTW = 32;  // words per update chunk (one per lane)
-constexpr int kRegThreads = 128;  // threads holding a panel in registers (m <= 1024)
-constexpr int kRegRows = 8;        // rows per thread there
+constexpr int kRegThreads = 256;  // threads holding a panel in registers (m <= 1024)
+constexpr int kRegRows = 4;        // rows per thread there
+constexpr int kRegWarps = kRegThreads / 32;
+static_assert(kRegWarps == 8, "eight candidate slots");
 constexpr int kRegBar = 6;         // their named barrier
 struct BigSmem {
     u64 coef[64];
-    u64 pub[2][4][2];      // per warp: its candidate pivot's panel word and tag (by bit parity)
-    alignas(16) unsigned wmin[2][4];  // per warp: its candidate pivot row
+    u64 pub[2][kRegWarps][2];  // per warp: its candidate pivot's panel word and tag (by bit parity)
+    alignas(16) unsigned wmin[2][kRegWarps];  // per warp: its candidate pivot row
     int bits[64], srow[64];
     int slots[4];
     u64 T[16][16][kTW];  // nibble tables of the current chunk
@@ -256,13 +258,11 @@ constexpr size_t kBigExtra = (size_t)kSmemTotal - ((sizeof(BigSmem) + 15) & ~(si
 static_assert(sizeof(BigSmem) <= (size_t)kSmemTotal, "big-matrix shared memory");
 }  // namespace
 
-// Element i (0..7, per thread) of a register array, by a select tree.
-__device__ __forceinline__ u64 sel8(const u64 (&v)[8], int i)
+// Element i (0..3, per thread) of a register array, by a select tree.
+__device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 {
-    const u64 a0 = (i & 1) ? v[1] : v[0], a1 = (i & 1) ? v[3] : v[2], a2 = (i & 1) ? v[5] : v[4],
-              a3 = (i & 1) ? v[7] : v[6];
-    const u64 b0 = (i & 2) ? a1 : a0, b1 = (i & 2) ? a3 : a2;
-    return (i & 4) ? b1 : b0;
+    const u64 a0 = (i & 1) ? v[1] : v[0], a1 = (i & 1) ? v[3] : v[2];
+    return (i & 2) ? a1 : a0;
 }
 
 // 32x32 bit transposes by warp shuffles over a CTA: dst (cols x rows bits,
@@ -341,10 +341,10 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         int k = 0;
         u64 pmask = 0;
         if (m <= kRegRows * kRegThreads) {
-            // 1-2. the panel in registers of the first four warps: thread l
-            // holds rows l + 128 i.  Per bit one named barrier: each warp
+            // 1-2. the panel in registers of the first eight warps: thread l
+            // holds rows l + 256 i.  Per bit one named barrier: each warp
             // publishes its lowest unused row holding the bit (index, panel
-            // word and tag); the lowest of the four is the pivot.
+            // word and tag); the lowest of the eight is the pivot.
             for (int j = tid; j < m; j += kThreads) ysnap[j] = A[(size_t)j * wc + w];
             __syncthreads();
             if (tid < kRegThreads) {
@@ -372,13 +372,15 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                         const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
                         const int par = bb & 1;
                         if (jb == wm && wm != (unsigned)INT_MAX) {
-                            S.pub[par][warp][0] = sel8(y, ib);
-                            S.pub[par][warp][1] = sel8(t, ib);
+                            S.pub[par][warp][0] = sel4r(y, ib);
+                            S.pub[par][warp][1] = sel4r(t, ib);
                         }
                         if (lane == 0) S.wmin[par][warp] = wm;
                         asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
-                        const uint4 wmv = *reinterpret_cast<const uint4 *>(S.wmin[par]);
-                        const unsigned pm = min(min(wmv.x, wmv.y), min(wmv.z, wmv.w));
+                        const uint4 wa = reinterpret_cast<const uint4 *>(S.wmin[par])[0];
+                        const uint4 wb = reinterpret_cast<const uint4 *>(S.wmin[par])[1];
+                        const unsigned pm = min(min(min(wa.x, wa.y), min(wa.z, wa.w)),
+                                                min(min(wb.x, wb.y), min(wb.z, wb.w)));
                         if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
                         const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
                         const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
