@@ -616,6 +616,38 @@ def elim_only():
     print(json.dumps(out))
 
 
+def batch_only(lo: int, hi: int, reps: int = 3):
+    """Profiling aid: the parity-check batch (seed 3) restricted to the matrices
+    with lo <= m < hi, packed input resident in HBM, one persistent launch per
+    run without a graph; prints the per-run time."""
+    import numpy as np
+    import torch
+    from mex_linear_algebra_b200 import device as D, gen
+    shapes, offsets, buf = gen.ldpc_batch(20000, 3)
+    sel = (shapes[:, 0] >= lo) & (shapes[:, 0] < hi)
+    idx = np.nonzero(sel)[0]
+    sh = shapes[sel]
+    wcs = (sh[:, 1] + 63) // 64
+    packed = np.concatenate([buf[offsets[i]:offsets[i] + shapes[i, 0] * w] for i, w in zip(idx, wcs)])
+    plan = D.BatchPlan(sh)
+    d = torch.from_numpy(packed.view(np.int64)).cuda()
+    ranks, zt = plan.outputs()
+    for _ in range(2):
+        plan.run(d, ranks, zt, use_graph=False)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.run(d, ranks, zt, use_graph=False)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"matrices": int(sel.sum()), "m_range": [lo, hi], "ms": round(min(times), 3),
+                      "classes": plan.stats()}))
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -633,10 +665,15 @@ def main():
     ap.add_argument("--elim-only", action="store_true",
                     help="profiling aid: build the dense rank configuration and run one rank and one "
                          "RREF with the tensor-core elimination form, print their times, nothing else")
+    ap.add_argument("--batch-only", nargs=2, type=int, metavar=("M_LO", "M_HI"),
+                    help="profiling aid: run the parity-check batch restricted to M_LO <= m < M_HI "
+                         "(packed input, no graph) and print its time, nothing else")
     args = ap.parse_args()
     set_size(args.size)
     if args.elim_only:
         return elim_only()
+    if args.batch_only:
+        return batch_only(*args.batch_only)
     from mex_linear_algebra_b200 import parallel
     ws, rank, local = parallel.world()
     if args.impl == "reference":
