@@ -257,6 +257,11 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
     base_rate = baseline_sample / t_base
     rate = count / (ms * 1e-3)
     in_bytes = plan.logical_bytes
+    # forward-elimination work (rank m, pivots in the leading columns) and the bytes that must move
+    ms_, ns_ = shapes[:, 0].astype(np.float64), shapes[:, 1].astype(np.float64)
+    work = float(sum(2.0 * ((mm - 1 - np.arange(mm)) * (nn - np.arange(mm))).sum()
+                     for mm, nn in zip(shapes[:, 0], shapes[:, 1])))
+    z_bytes = float(((ns_ - ms_) * ((ns_ + 63) // 64) * 8).sum())
     classes = plan.stats()
     plan.close()
     return {"metric": "batched rank+null mats/s", "value": round(rate, 1), "unit": "matrices/s",
@@ -268,7 +273,14 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
                                  "sample": f"{baseline_sample} matrices spread over the batch, "
                                            "pack-free packed input, plain RREF + null basis per matrix, "
                                            "host clock per matrix"},
-            "speedup_vs_per_matrix": round(rate / base_rate, 1), "results_match": ok}
+            "speedup_vs_per_matrix": round(rate / base_rate, 1), "results_match": ok,
+            "roofline": {"bound": "bit-op issue (shared memory / barrier chain), not HBM",
+                         "work_tbitop": round(work / 1e12, 3),
+                         "achieved_tbitops": round(work / (ms * 1e-3) / 1e12, 1),
+                         "hbm_bytes": in_bytes + z_bytes,
+                         "hbm_gbs": round((in_bytes + z_bytes) / (ms * 1e-3) / 1e9, 1),
+                         "work_note": "sum over matrices of sum_p 2(m-p-1)(n-p): forward elimination "
+                                      "with the pivots in the leading columns"}}
 
 
 def bench_dense_rank(torch):
