@@ -628,10 +628,10 @@ def elim_only():
     print(json.dumps(out))
 
 
-def batch_only(lo: int, hi: int, reps: int = 3):
+def batch_only(lo: int, hi: int, logical: bool = False, reps: int = 3):
     """Profiling aid: the parity-check batch (seed 3) restricted to the matrices
-    with lo <= m < hi, packed input resident in HBM, one persistent launch per
-    run without a graph; prints the per-run time."""
+    with lo <= m < hi, packed (or, with `logical`, MATLAB logical) input
+    resident in HBM, launched without a graph; prints the per-run time."""
     import numpy as np
     import torch
     from mex_linear_algebra_b200 import device as D, gen
@@ -644,18 +644,22 @@ def batch_only(lo: int, hi: int, reps: int = 3):
     plan = D.BatchPlan(sh)
     d = torch.from_numpy(packed.view(np.int64)).cuda()
     ranks, zt = plan.outputs()
+    if logical:
+        d = plan.unpack_logical(d)
+    run = plan.run_logical if logical else plan.run
     for _ in range(2):
-        plan.run(d, ranks, zt, use_graph=False)
+        run(d, ranks, zt, use_graph=False)
     torch.cuda.synchronize()
     times = []
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        plan.run(d, ranks, zt, use_graph=False)
+        run(d, ranks, zt, use_graph=False)
         e1.record()
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
-    print(json.dumps({"matrices": int(sel.sum()), "m_range": [lo, hi], "ms": round(min(times), 3),
+    print(json.dumps({"matrices": int(sel.sum()), "m_range": [lo, hi], "input": "logical" if logical else "packed",
+                      "ms": round(min(times), 3),
                       "classes": plan.stats()}))
     plan.close()
 
@@ -680,12 +684,14 @@ def main():
     ap.add_argument("--batch-only", nargs=2, type=int, metavar=("M_LO", "M_HI"),
                     help="profiling aid: run the parity-check batch restricted to M_LO <= m < M_HI "
                          "(packed input, no graph) and print its time, nothing else")
+    ap.add_argument("--batch-logical", action="store_true",
+                    help="with --batch-only: start from the MATLAB logical input instead")
     args = ap.parse_args()
     set_size(args.size)
     if args.elim_only:
         return elim_only()
     if args.batch_only:
-        return batch_only(*args.batch_only)
+        return batch_only(*args.batch_only, logical=args.batch_logical)
     from mex_linear_algebra_b200 import parallel
     ws, rank, local = parallel.world()
     if args.impl == "reference":

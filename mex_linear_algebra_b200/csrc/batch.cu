@@ -678,54 +678,121 @@ batch_kernel(const BatchDevItem *__restrict__ items, const int *__restrict__ ord
     }
 }
 
-// logical column-major inputs -> packed rows, for every matrix of the batch
-__global__ void batch_pack_kernel(const BatchDevItem *__restrict__ items, const long long *byte_off,
-                                  const long long *tile_start, int count,
-                                  const unsigned char *__restrict__ in, u64 *__restrict__ out)
+// Logical <-> packed tiles: a block covers one word column (64 columns) of
+// up to kPackRows rows of one matrix (tile_mat names the matrix; tile -
+// tile_start[matrix] = row chunk * wc + word).  In the column-major logical
+// layout each column's rows are contiguous, so the block reads 64 runs of up
+// to kPackRows bytes.
+constexpr int kPackRows = 512;  // 64 staged runs of up to 512 bytes: 34 KB of shared memory
+constexpr int kPackPitch = kPackRows + 32;  // bytes per staged column (16-byte alignment slack)
+
+// logical column-major inputs -> packed rows, for every matrix of the batch:
+// the 64 column runs land in shared memory by aligned 16-byte loads (each run
+// keeps its offset within its first 16 bytes), then thread t builds the
+// words of rows t, t + 256, ... from 64 bytes each (nonzero -> 1).
+__global__ void __launch_bounds__(256) batch_pack_kernel(const BatchDevItem *__restrict__ items,
+                                                         const long long *byte_off,
+                                                         const long long *tile_start,
+                                                         const int *__restrict__ tile_mat,
+                                                         const unsigned char *__restrict__ in, long long total,
+                                                         u64 *__restrict__ out)
 {
-    // one block = 32 rows x 8 words of one matrix; find the matrix by binary search
+    __shared__ __align__(16) unsigned char col[64][kPackPitch];
+    __shared__ int off[64];
     const long long b = blockIdx.x;
-    int lo = 0, hi = count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_start[mid] <= b) lo = mid; else hi = mid - 1;
-    }
+    const int lo = tile_mat[b];
     const BatchDevItem it = items[lo];
     const long long tile = b - tile_start[lo];
-    const int wc = (it.n + 63) >> 6, wg = (wc + 7) / 8;
-    const int rt = (int)(tile / wg), wt = (int)(tile % wg);
-    const int lane = threadIdx.x & 31, w8 = threadIdx.x >> 5;
-    const int row = rt * 32 + lane, w = wt * 8 + w8;
-    if (row >= it.m || w >= wc) return;
-    const unsigned char *p = in + byte_off[lo] + row + (long long)w * 64 * it.m;
+    const int wc = (it.n + 63) >> 6;
+    const int rc = (int)(tile / wc), w = (int)(tile % wc);
+    const int r0 = rc * kPackRows;
+    const int rows = (it.m - r0) < kPackRows ? (it.m - r0) : kPackRows;
     const int cols = (it.n - w * 64) < 64 ? (it.n - w * 64) : 64;
-    u64 word = 0;
-    for (int j = 0; j < cols; ++j) word |= (u64)(p[(long long)j * it.m] != 0) << j;
-    out[it.in_off + (long long)row * wc + w] = word;
+    const long long base = byte_off[lo] + (long long)w * 64 * it.m + r0;
+    const int chunks = (rows + 15 + 15) / 16;  // 16-byte pieces covering a run at any alignment
+    {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int c = warp; c < cols; c += 8) {  // a warp per run, a lane per 16 bytes
+            const long long g = base + (long long)c * it.m;
+            if (lane == 0) off[c] = (int)(g & 15);
+            for (int q = lane; q < chunks; q += 32) {
+                const long long a = (g & ~15LL) + 16LL * q;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (a + 16 <= total) {
+                    v = *reinterpret_cast<const uint4 *>(in + a);
+                } else if (a < total) {
+                    unsigned char t[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) t[i] = (a + i < total) ? in[a + i] : 0;
+                    v = *reinterpret_cast<const uint4 *>(t);
+                }
+                *reinterpret_cast<uint4 *>(&col[c][16 * q]) = v;
+            }
+        }
+    }
+    __syncthreads();
+    // warps 0-3 take columns 0-31, warps 4-7 columns 32-63; lane l of warp
+    // w4 = warp & 3 takes rows 128 w4 + 4 l .. + 3 as one 32-bit read per
+    // column (two aligned reads funnel-shifted by the run's offset), folds
+    // each byte to its bit 0 (nonzero) and gathers 8 columns per word: byte k
+    // of that word holds row k's bits for the 8 columns
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chalf = warp >> 2, w4 = warp & 3;
+    const int rl = 128 * w4 + 4 * lane;  // first of this lane's rows in the tile
+    u32 half[4] = {0, 0, 0, 0};
+    if (rl < rows) {
+#pragma unroll
+        for (int ob = 0; ob < 4; ++ob) {
+            u32 oct = 0;
+#pragma unroll
+            for (int cc = 0; cc < 8; ++cc) {
+                const int c = 32 * chalf + 8 * ob + cc;
+                if (c < cols) {
+                    const int o = off[c] + rl;
+                    const u32 *p32 = reinterpret_cast<const u32 *>(&col[c][o & ~3]);
+                    const u32 v = __funnelshift_r(p32[0], p32[1], 8 * (o & 3));
+                    u32 t = v | (v >> 4);
+                    t |= t >> 2;
+                    t |= t >> 1;
+                    oct |= (t & 0x01010101u) << cc;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) half[k] |= ((oct >> (8 * k)) & 0xFFu) << (8 * ob);
+        }
+    }
+    u32 *out32 = reinterpret_cast<u32 *>(out);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = rl + k;
+        if (r < rows && 32 * chalf < cols) out32[2 * (it.in_off + (long long)(r0 + r) * wc + w) + chalf] = half[k];
+        else if (r < rows && chalf == 1) out32[2 * (it.in_off + (long long)(r0 + r) * wc + w) + 1] = 0u;
+    }
 }
 
 // packed rows -> logical column-major inputs, for every matrix of the batch
-__global__ void batch_unpack_kernel(const BatchDevItem *__restrict__ items, const long long *byte_off,
-                                    const long long *tile_start, int count, const u64 *__restrict__ in,
-                                    unsigned char *__restrict__ out)
+// (same tiles; thread t writes the 64 bytes of rows t, t + 256, ...)
+__global__ void __launch_bounds__(256) batch_unpack_kernel(const BatchDevItem *__restrict__ items,
+                                                           const long long *byte_off,
+                                                           const long long *tile_start,
+                                                           const int *__restrict__ tile_mat,
+                                                           const u64 *__restrict__ in,
+                                                           unsigned char *__restrict__ out)
 {
     const long long b = blockIdx.x;
-    int lo = 0, hi = count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_start[mid] <= b) lo = mid; else hi = mid - 1;
-    }
+    const int lo = tile_mat[b];
     const BatchDevItem it = items[lo];
     const long long tile = b - tile_start[lo];
-    const int wc = (it.n + 63) >> 6, wg = (wc + 7) / 8;
-    const int rt = (int)(tile / wg), wt = (int)(tile % wg);
-    const int lane = threadIdx.x & 31, w8 = threadIdx.x >> 5;
-    const int row = rt * 32 + lane, w = wt * 8 + w8;
-    if (row >= it.m || w >= wc) return;
-    const u64 word = in[it.in_off + (long long)row * wc + w];
-    unsigned char *p = out + byte_off[lo] + row + (long long)w * 64 * it.m;
+    const int wc = (it.n + 63) >> 6;
+    const int rc = (int)(tile / wc), w = (int)(tile % wc);
+    const int r0 = rc * kPackRows;
+    const int rows = (it.m - r0) < kPackRows ? (it.m - r0) : kPackRows;
     const int cols = (it.n - w * 64) < 64 ? (it.n - w * 64) : 64;
-    for (int j = 0; j < cols; ++j) p[(long long)j * it.m] = (unsigned char)((word >> j) & 1);
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+        const u64 word = in[it.in_off + (long long)(r0 + r) * wc + w];
+        unsigned char *p = out + byte_off[lo] + (long long)w * 64 * it.m + r0 + r;
+        for (int j = 0; j < cols; ++j) p[(long long)j * it.m] = (unsigned char)((word >> j) & 1);
+    }
 }
 
 // ---------------------------------------------------------------- single matrix
@@ -794,7 +861,9 @@ struct BatchPlanImpl {
     int grid = 0;
     // logical-input path
     long long *d_byte_off = nullptr, *d_tile_start = nullptr;
+    int *d_tile_mat = nullptr;  // matrix of each packing tile
     long long pack_tiles = 0;
+    long long logical_total = 0;  // bytes of the logical input
     u64 *d_packed = nullptr;
     long long packed_words = 0;
     // CUDA graph of the last run
@@ -818,6 +887,7 @@ static mela_status plan_free(BatchPlanImpl *P)
     cudaFree(P->d_gscratch);
     cudaFree(P->d_byte_off);
     cudaFree(P->d_tile_start);
+    cudaFree(P->d_tile_mat);
     cudaFree(P->d_packed);
     delete P;
     return MELA_OK;
@@ -891,10 +961,16 @@ static mela_status plan_create(const mela_batch_item *h, long long count, int fo
         boff += h[i].m * h[i].n;
         tiles[(size_t)i] = t;
         const long long wc = (h[i].n + 63) / 64;
-        t += ((h[i].m + 31) / 32) * ((wc + 7) / 8);
+        t += ((h[i].m + kPackRows - 1) / kPackRows) * wc;
         P->packed_words = std::max(P->packed_words, h[i].in_offset + h[i].m * wc);
     }
     P->pack_tiles = t;
+    P->logical_total = boff;
+    std::vector<int> tile_mat((size_t)(t > 0 ? t : 1), 0);
+    for (long long i = 0; i < count; ++i) {
+        const long long end = i + 1 < count ? tiles[(size_t)i + 1] : t;
+        for (long long q = tiles[(size_t)i]; q < end; ++q) tile_mat[(size_t)q] = (int)i;
+    }
 
     auto dmal = [&](void **p, size_t bytes) -> mela_status {
         cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
@@ -907,14 +983,16 @@ static mela_status plan_create(const mela_batch_item *h, long long count, int fo
         (st = dmal((void **)&P->d_counters, 4 * sizeof(int))) != MELA_OK ||
         (st = dmal((void **)&P->d_gscratch, (size_t)P->grid * (size_t)max_big_words * 8)) != MELA_OK ||
         (st = dmal((void **)&P->d_byte_off, byte_off.size() * 8)) != MELA_OK ||
-        (st = dmal((void **)&P->d_tile_start, tiles.size() * 8)) != MELA_OK) {
+        (st = dmal((void **)&P->d_tile_start, tiles.size() * 8)) != MELA_OK ||
+        (st = dmal((void **)&P->d_tile_mat, tile_mat.size() * 4)) != MELA_OK) {
         plan_free(P);
         return st;
     }
     cudaMemcpy(P->d_items, items.data(), items.size() * sizeof(BatchDevItem), cudaMemcpyHostToDevice);
     cudaMemcpy(P->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(P->d_byte_off, byte_off.data(), byte_off.size() * 8, cudaMemcpyHostToDevice);
-    cudaError_t e = cudaMemcpy(P->d_tile_start, tiles.data(), tiles.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(P->d_tile_start, tiles.data(), tiles.size() * 8, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(P->d_tile_mat, tile_mat.data(), tile_mat.size() * 4, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         plan_free(P);
         return cuda_status(e, "batch plan upload");
@@ -939,8 +1017,8 @@ static mela_status enqueue_logical(BatchPlanImpl *P, const unsigned char *in, u6
 {
     if (P->count && P->pack_tiles) {
         batch_pack_kernel<<<(unsigned)P->pack_tiles, 256, 0, s>>>(P->d_items, P->d_byte_off,
-                                                                   P->d_tile_start, P->count, in,
-                                                                   P->d_packed);
+                                                                   P->d_tile_start, P->d_tile_mat, in,
+                                                                   P->logical_total, P->d_packed);
         MELA_LAUNCH_CHECK("batch_pack_kernel");
     }
     return enqueue(P, P->d_packed, zt, ranks, s);
@@ -1053,7 +1131,7 @@ extern "C" mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const ui
     BatchPlanImpl *P = plan->impl;
     if (P->count && P->pack_tiles) {
         batch_unpack_kernel<<<(unsigned)P->pack_tiles, 256, 0, (cudaStream_t)stream>>>(
-            P->d_items, P->d_byte_off, P->d_tile_start, P->count, (const u64 *)d_packed, d_logical);
+            P->d_items, P->d_byte_off, P->d_tile_start, P->d_tile_mat, (const u64 *)d_packed, d_logical);
         MELA_LAUNCH_CHECK("batch_unpack_kernel");
     }
     return MELA_OK;
