@@ -24,7 +24,8 @@
 //                   the list is then compacted in place (pivot rows and rows
 //                   found zero from the window on are dropped, order kept).
 //   window_combine  R_t = sum_j T[t][j] A[P_j] over the words from the window
-//                   on, into the panel buffer (a warp per t, a lane per word).
+//                   on, into the panel buffer (a block per 4 words, 4-bit
+//                   tables over the P rows).
 //   window_coef     every other row to update (rank: the active rows; RREF: all
 //                   rows) whose bits at the window's pivot columns are not all
 //                   zero gets a slot; those bits become a row of 0/1 bytes.
@@ -32,10 +33,10 @@
 //                   R_t written over row P_t.
 //   tc_update       A[row(slot), w..] ^= parity(X8[slot] . Rt8^T): tcgen05
 //                   kind::i8 128 x 256 tiles with K = 256.  A persistent CTA
-//                   keeps 256-column strips of Rt8 in shared memory (two
-//                   buffers) and streams 128-row tiles of X8 through a 2-stage
-//                   ring into two TMEM accumulators; four epilogue warps XOR the
-//                   parity bits into the packed rows while the next tile is
+//                   keeps a 256-column strip of Rt8 in shared memory and
+//                   streams 128-row tiles of X8 through a 4-stage ring into two
+//                   TMEM accumulators; sixteen epilogue warps XOR the parity
+//                   bits into the packed rows while the next tile is
 //                   multiplied, and flag the rows that are still nonzero.
 // Since the basis is reduced, a row's coefficient for R_t is its own bit at
 // pivot column t, and XORing sum_t x_t R_t clears every pivot column of the
