@@ -330,6 +330,10 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u64 *ysnap = rows_in_smem ? reinterpret_cast<u64 *>(extra + used) : g + L.ysg;
     u64 *yv = rows_in_smem ? ysnap + m : g + L.yvg;
     u64 *tag = rows_in_smem ? yv + m : g + L.tagg;
+    if (rows_in_smem) used += 3 * row_bytes;
+    // the matrix itself in shared memory too when it fits (m up to about 650
+    // at n = 2m), else in the CTA's L2-resident scratch
+    if (used + (size_t)m * wc * 8 <= kBigExtra) A = reinterpret_cast<u64 *>(extra + used);
 
     const u64 *src = in + it.in_off;
     for (long long e = tid; e < (long long)m * wc; e += kThreads) A[e] = src[e];
