@@ -312,7 +312,12 @@ def bench_dense_rank(torch):
     ranks = set()
     for form in ("tc", "m4ri", "m4ri_k4", "plain"):
         v = _lib.ELIM_VARIANTS[form]
+        # one untimed call first: one-time costs (the tensor-core form captures
+        # its launch sequence into a CUDA graph on the first call)
         Mx = A.clone()
+        check(L.mela_dev_rank(v, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                              ws.data_ptr(), wsb, s))
+        Mx.copy_(A)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -345,6 +350,9 @@ def bench_dense_rank(torch):
     out["null_ms"]["m4ri_rref"] = round(e0.elapsed_time(e1), 2)
     rows_m4ri = Mx[dpr[:int(dr.item())]].clone()
     Mx = A.clone()
+    check(L.mela_dev_rref(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                          dpr.data_ptr(), ws.data_ptr(), wsb, s))  # untimed first call
+    Mx.copy_(A)
     torch.cuda.synchronize()
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     e0.record()
@@ -596,7 +604,7 @@ def run_mela(args, ws, rank, local):
 
 
 def elim_only():
-    """One rank and one RREF of the 16384 x 32768 rank-12000 configuration by the
+    """A rank and an RREF (each after one untimed call) of the 16384 x 32768 rank-12000 configuration by the
     tensor-core elimination form (the dense section's inputs), for profiling."""
     import torch
     from mex_linear_algebra_b200 import device as D, gen, _lib
@@ -616,6 +624,9 @@ def elim_only():
     out = {}
     for name, fn in (("rank", L.mela_dev_rank), ("rref", L.mela_dev_rref)):
         Mx = A.clone()
+        check(fn(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                 ws.data_ptr(), wsb, s))  # untimed first call
+        Mx.copy_(A)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()

@@ -82,6 +82,7 @@ struct HostCtx {
     cudaStream_t copy_in[kMaxDevices] = {};   // pipelined host products: uploads
     cudaStream_t copy_out[kMaxDevices] = {};  //   and downloads
     cudaStream_t side[kMaxDevices] = {};      // work forked off a caller's stream
+    cudaStream_t capture[kMaxDevices] = {};   // origin of graph captures
 };
 static thread_local HostCtx t_ctx;
 
@@ -122,6 +123,14 @@ mela_status side_stream(cudaStream_t *s)
     const int d = current_device();
     if (!t_ctx.side[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.side[d], cudaStreamNonBlocking));
     *s = t_ctx.side[d];
+    return MELA_OK;
+}
+
+mela_status capture_stream(cudaStream_t *s)
+{
+    const int d = current_device();
+    if (!t_ctx.capture[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.capture[d], cudaStreamNonBlocking));
+    *s = t_ctx.capture[d];
     return MELA_OK;
 }
 
