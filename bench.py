@@ -312,11 +312,13 @@ def bench_dense_rank(torch):
     ranks = set()
     for form in ("tc", "m4ri", "m4ri_k4", "plain"):
         v = _lib.ELIM_VARIANTS[form]
-        # one untimed call first: one-time costs (the tensor-core form captures
-        # its launch sequence into a CUDA graph on the first call)
+        # untimed calls first: one-time costs (the tensor-core form captures its
+        # launch sequence into a CUDA graph on the second call with the same buffers)
         Mx = A.clone()
-        check(L.mela_dev_rank(v, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
-                              ws.data_ptr(), wsb, s))
+        for _ in range(2 if form == "tc" else 1):
+            Mx.copy_(A)
+            check(L.mela_dev_rank(v, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                                  ws.data_ptr(), wsb, s))
         Mx.copy_(A)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -350,8 +352,10 @@ def bench_dense_rank(torch):
     out["null_ms"]["m4ri_rref"] = round(e0.elapsed_time(e1), 2)
     rows_m4ri = Mx[dpr[:int(dr.item())]].clone()
     Mx = A.clone()
-    check(L.mela_dev_rref(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
-                          dpr.data_ptr(), ws.data_ptr(), wsb, s))  # untimed first call
+    for _ in range(2):  # untimed calls (the second captures the CUDA graph)
+        Mx.copy_(A)
+        check(L.mela_dev_rref(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                              dpr.data_ptr(), ws.data_ptr(), wsb, s))
     Mx.copy_(A)
     torch.cuda.synchronize()
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -604,7 +608,7 @@ def run_mela(args, ws, rank, local):
 
 
 def elim_only():
-    """A rank and an RREF (each after one untimed call) of the 16384 x 32768 rank-12000 configuration by the
+    """Three ranks and three RREFs (first call, graph capture, replay) of the 16384 x 32768 rank-12000 configuration by the
     tensor-core elimination form (the dense section's inputs), for profiling."""
     import torch
     from mex_linear_algebra_b200 import device as D, gen, _lib
@@ -624,17 +628,20 @@ def elim_only():
     out = {}
     for name, fn in (("rank", L.mela_dev_rank), ("rref", L.mela_dev_rref)):
         Mx = A.clone()
-        check(fn(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
-                 ws.data_ptr(), wsb, s))  # untimed first call
-        Mx.copy_(A)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        check(fn(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
-                 ws.data_ptr(), wsb, s))
-        e1.record()
-        e1.synchronize()
-        out[name + "_ms"] = round(e0.elapsed_time(e1), 3)
+        calls = []
+        for _ in range(3):  # first call, graph capture, replay
+            Mx.copy_(A)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            check(fn(_lib.ELIM_TC, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(), dpr.data_ptr(),
+                     ws.data_ptr(), wsb, s))
+            e1.record()
+            e1.synchronize()
+            calls.append((round(e0.elapsed_time(e1), 3), round((time.perf_counter() - t0) * 1e3, 3)))
+        out[name + "_ms"] = calls[-1][0]
+        out[name + "_calls_device_host_ms"] = calls
         out[name] = int(dr.item())
     print(json.dumps(out))
 

@@ -945,8 +945,10 @@ struct ElimGraph {
     cudaGraphExec_t exec;
 };
 constexpr size_t kMaxElimGraphs = 16;
+constexpr size_t kMaxElimSeen = 64;
 std::mutex g_elim_graph_mu;
 std::vector<ElimGraph> *g_elim_graphs = nullptr;
+std::vector<ElimGraphKey> *g_elim_seen = nullptr;  // calls made once, without a graph
 
 bool elim_graphs_enabled()
 {
@@ -962,9 +964,10 @@ cudaGraphExec_t elim_graph_lookup(const ElimGraphKey &k)
         if (std::memcmp(&g.k, &k, sizeof k) == 0) return g.exec;
     return nullptr;
 }
-// The stream is not being captured by the caller and there is room to keep
-// one more graph.
-bool elim_graph_capturable(cudaStream_t s)
+// Capture now: the same call (device, buffers, shape, form) was made before
+// -- a one-off call does not pay for instantiating a graph --, the stream is
+// not being captured by the caller and there is room to keep one more graph.
+bool elim_graph_capturable(const ElimGraphKey &k, cudaStream_t s)
 {
     if (!elim_graphs_enabled()) return false;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -973,7 +976,12 @@ bool elim_graph_capturable(cudaStream_t s)
         return false;
     }
     std::lock_guard<std::mutex> lk(g_elim_graph_mu);
-    return !g_elim_graphs || g_elim_graphs->size() < kMaxElimGraphs;
+    if (g_elim_graphs && g_elim_graphs->size() >= kMaxElimGraphs) return false;
+    if (!g_elim_seen) g_elim_seen = new std::vector<ElimGraphKey>();
+    for (const ElimGraphKey &q : *g_elim_seen)
+        if (std::memcmp(&q, &k, sizeof k) == 0) return true;
+    if (g_elim_seen->size() < kMaxElimSeen) g_elim_seen->push_back(k);
+    return false;
 }
 void elim_graph_store(const ElimGraphKey &k, cudaGraphExec_t exec)
 {
@@ -1097,9 +1105,10 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
         MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &last->rank, sizeof(long long), cudaMemcpyDeviceToDevice, sx));
         return MELA_OK;
     };
-    // The launch sequence depends only on the shape and the buffers, so it is
-    // captured once into a CUDA graph per (device, buffers, shape, form), on
-    // the thread's capture stream, and replayed on the caller's stream: about
+    // The launch sequence depends only on the shape and the buffers, so from
+    // the second call on it is captured once into a CUDA graph per (device,
+    // buffers, shape, form), on the thread's capture stream, and replayed on
+    // the caller's stream: about
     // 1.4 ms less per 16384 x 32768 call than launching the 770 kernels and
     // events one by one.  A caller that is itself capturing gets the launches
     // in its own graph.
@@ -1120,7 +1129,7 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     if (exec) {
         st = cudaGraphLaunch(exec, s) == cudaSuccess ? MELA_OK : MELA_ERR_CUDA;
         if (st != MELA_OK) set_error("cudaGraphLaunch (tensor-core elimination) failed");
-    } else if (elim_graph_capturable(s) && capture_stream(&cap) == MELA_OK) {
+    } else if (elim_graph_capturable(key, s) && capture_stream(&cap) == MELA_OK) {
         st = MELA_OK;
         if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
