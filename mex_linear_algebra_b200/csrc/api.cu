@@ -83,6 +83,7 @@ struct HostCtx {
     cudaStream_t copy_out[kMaxDevices] = {};  //   and downloads
     cudaStream_t side[kMaxDevices] = {};      // work forked off a caller's stream
     cudaStream_t capture[kMaxDevices] = {};   // origin of graph captures
+    cudaStream_t aux[kMaxDevices] = {};       // a second fork off a caller's stream
 };
 static thread_local HostCtx t_ctx;
 
@@ -123,6 +124,14 @@ mela_status side_stream(cudaStream_t *s)
     const int d = current_device();
     if (!t_ctx.side[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.side[d], cudaStreamNonBlocking));
     *s = t_ctx.side[d];
+    return MELA_OK;
+}
+
+mela_status aux_stream(cudaStream_t *s)
+{
+    const int d = current_device();
+    if (!t_ctx.aux[d]) MELA_CUDA_TRY(cudaStreamCreateWithFlags(&t_ctx.aux[d], cudaStreamNonBlocking));
+    *s = t_ctx.aux[d];
     return MELA_OK;
 }
 

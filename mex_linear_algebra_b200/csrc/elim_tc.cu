@@ -1022,6 +1022,8 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     if (st != MELA_OK) return st;
     cudaStream_t s2;
     if ((st = side_stream(&s2)) != MELA_OK) return st;
+    cudaStream_t s3;  // the coefficient pass, beside the combine and transpose
+    if ((st = aux_stream(&s3)) != MELA_OK) return st;
 
     const size_t wf_smem = sizeof(WfSmem);
     MELA_CUDA_TRY(cudaFuncSetAttribute(window_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1043,13 +1045,19 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     // and its coefficient and R buffers are the ones the rest still reads.
     // Window states and row flags alternate by window parity so that the
     // factorization of w+1 never writes what the update of w reads.
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    MELA_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    if (cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess) {
-        cudaEventDestroy(ev_fork);
-        set_error("cudaEventCreate failed");
-        return MELA_ERR_CUDA;
+    // The coefficient pass of a window reads only rows that are not its pivot
+    // rows, which the transpose kernel overwrites, so it runs on a third
+    // stream beside the combine and the transpose and rejoins before the
+    // update.
+    cudaEvent_t evs[4] = {};
+    for (int i = 0; i < 4; ++i) {
+        if (cudaEventCreateWithFlags(&evs[i], cudaEventDisableTiming) != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaEventDestroy(evs[j]);
+            set_error("cudaEventCreate failed");
+            return MELA_ERR_CUDA;
+        }
     }
+    cudaEvent_t ev_fork = evs[0], ev_join = evs[1], ev_cfork = evs[2], ev_cjoin = evs[3];
     cudaStream_t sx = s;  // the stream the launches go to (a capture stream while capturing)
     auto run = [&]() -> mela_status {
         MELA_CUDA_TRY(cudaMemsetAsync(state, 1, (size_t)m, sx));
@@ -1069,11 +1077,15 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
                 MELA_CUDA_TRY(cudaStreamWaitEvent(sx, ev_join, 0));
                 forked = false;
             }
+            MELA_CUDA_TRY(cudaEventRecord(ev_cfork, sx));
+            MELA_CUDA_TRY(cudaStreamWaitEvent(s3, ev_cfork, 0));
+            window_coef_kernel<<<coef_blocks, 256, 0, s3>>>(M, ld, m, wc, w, list, stamp, wid, rref, cur, ulist, X8,
+                                                           live);
+            MELA_CUDA_TRY(cudaEventRecord(ev_cjoin, s3));
             window_combine_kernel<<<(unsigned)((lw + CB_W - 1) / CB_W), 256, cb_smem, sx>>>(M, ld, wc, w, cur, Rbuf,
                                                                                            wc);
-            window_coef_kernel<<<coef_blocks, 256, 0, sx>>>(M, ld, m, wc, w, list, stamp, wid, rref, cur, ulist, X8,
-                                                           live);
             window_rt_kernel<<<(unsigned)lw, 256, 0, sx>>>(M, ld, w, Rbuf, wc, cur, Rt8);
+            MELA_CUDA_TRY(cudaStreamWaitEvent(sx, ev_cjoin, 0));
             // near: strip 1 (the next window's columns, all the next
             // factorization reads), one row tile per CTA; far: strip 0 (the
             // window's own columns: only the RREF needs them -- for the rank
@@ -1154,8 +1166,7 @@ mela_status elim_tc_device(u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_
     } else {
         st = run();
     }
-    cudaEventDestroy(ev_fork);
-    cudaEventDestroy(ev_join);
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
     return st;
 }
 

@@ -22,6 +22,8 @@ mela_status host_stream(cudaStream_t *s);
 // The calling thread's side stream on the current device: work forked from a
 // caller's stream (through an event) and joined back to it before returning.
 mela_status side_stream(cudaStream_t *s);
+// A second side stream of the calling thread, for work forked beside the first.
+mela_status aux_stream(cudaStream_t *s);
 // The calling thread's stream for capturing launch sequences into CUDA graphs
 // (a graph is captured there and launched on the caller's stream).
 mela_status capture_stream(cudaStream_t *s);
