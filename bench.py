@@ -395,10 +395,12 @@ def bench_dispatch(torch, count=200):
     if not os.path.exists(costmodel.DEFAULT_MODEL):
         return {"unavailable": "no trained cost model installed"}
     params = costmodel.load()
-    recs = autotune.build_db(count, 200000, reps=2, max_cells=2e7)
+    # median of 3 after a warm-up: the tensor-core elimination captures its
+    # CUDA graph on the second call with the same buffers (the first timed one)
+    recs = autotune.build_db(count, 200000, reps=3, max_cells=2e7)
     rep = costmodel.evaluate(params, recs)
     rep["sample"] = f"{len(recs)} requests of the mixed stream (seed 4) from request 200000, " \
-                    "each variant timed (median of 2 after a warm-up)"
+                    "each variant timed (median of 3 after a warm-up)"
     rep["all_variants_bit_identical"] = all(r["agree"] for r in recs)
     return rep
 
