@@ -131,7 +131,7 @@ def heuristic(op: str, m: int, n: int, p: int, density: float) -> str:
         if m >= 1024 and n >= 1024 and p >= 1024:
             return "tc_fp4" if n < (1 << 23) else "tc"
         return "plain"
-    return "fused" if m * n < 65536 else "tc"
+    return "fused" if m * n < 8192 else "tc"
 
 
 def evaluate(params: np.ndarray, records):

@@ -550,7 +550,7 @@ int choose_elim_variant(i64 m, i64 n, int rref)
     static const int order[5] = {MELA_ELIM_PLAIN, MELA_ELIM_M4RI, MELA_ELIM_M4RI_K4, MELA_ELIM_FUSED, MELA_ELIM_TC};
     if (c >= 0 && c < 5) return order[c];
     // fixed rule: one CTA for small matrices, tensor-core windows otherwise
-    return (double)m * (double)n < 65536.0 ? MELA_ELIM_FUSED : MELA_ELIM_TC;
+    return (double)m * (double)n < 8192.0 ? MELA_ELIM_FUSED : MELA_ELIM_TC;
 }
 
 mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank,
