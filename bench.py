@@ -220,6 +220,17 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    # the packing step alone (logical bytes -> packed rows), same input
+    d_pk = torch.zeros(max(plan.in_words, 1), dtype=torch.int64, device="cuda")
+    plan.pack_logical(d_log, d_pk)
+    e0.record()
+    for _ in range(reps):
+        plan.pack_logical(d_log, d_pk)
+    e1.record()
+    e1.synchronize()
+    pack_ms = e0.elapsed_time(e1) / reps
+    pack_ok = bool(torch.equal(d_pk, d_packed))
+    del d_pk
     # plain per-matrix path: pack, RREF (plain form), null basis, one matrix at a time
     L = lib()
     s = torch.cuda.current_stream().cuda_stream
@@ -274,6 +285,9 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
                                            "pack-free packed input, plain RREF + null basis per matrix, "
                                            "host clock per matrix"},
             "speedup_vs_per_matrix": round(rate / base_rate, 1), "results_match": ok,
+            "pack": {"ms": round(pack_ms, 3), "exact": pack_ok,
+                     "gbs": round((in_bytes + plan.in_words * 8) / (pack_ms * 1e-3) / 1e9, 1),
+                     "note": "batch_pack_kernel alone: logical bytes read + packed words written"},
             "roofline": {"bound": "bit-op issue (shared memory / barrier chain), not HBM",
                          "work_tbitop": round(work / 1e12, 3),
                          "achieved_tbitops": round(work / (ms * 1e-3) / 1e12, 1),

@@ -300,6 +300,13 @@ mela_status mela_batch_rank_null(mela_batch_plan *plan, const uint64_t *d_in, ui
 mela_status mela_batch_rank_null_logical(mela_batch_plan *plan, const uint8_t *d_in,
                                          uint64_t *d_zt, int64_t *d_ranks, int32_t use_graph,
                                          void *stream);
+/* Every matrix of the batch from its logical column-major form (the byte
+ * layout of the logical entry point, any alignment; nonzero bytes read as 1)
+ * to packed rows in the in_offset layout: the packing step of
+ * mela_batch_rank_null_logical on its own.  Words between the matrices are
+ * not written. */
+mela_status mela_batch_pack_logical(mela_batch_plan *plan, const uint8_t *d_logical,
+                                    uint64_t *d_packed, void *stream);
 /* Every matrix of the batch from packed rows (in_offset layout) to its
  * logical column-major form (the byte layout of the logical entry point). */
 mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_packed,

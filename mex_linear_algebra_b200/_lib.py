@@ -97,6 +97,7 @@ SIGNATURES = {
     "mela_batch_plan_stats": (_st, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "mela_batch_rank_null": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
     "mela_batch_rank_null_logical": (_st, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "mela_batch_pack_logical": (_st, [_vp, _vp, _vp, _vp]),
     "mela_batch_unpack_logical": (_st, [_vp, _vp, _vp, _vp]),
     "mela_mlp_forward": (_st, [_vp, _vp, _i64, _vp, _vp]),
     "mela_mlp_gradient": (_st, [_vp, _vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp]),

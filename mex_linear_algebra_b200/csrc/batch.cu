@@ -687,21 +687,53 @@ batch_kernel(const BatchDevItem *__restrict__ items, const int *__restrict__ ord
 // tile_start[matrix] = row chunk * wc + word).  In the column-major logical
 // layout each column's rows are contiguous, so the block reads 64 runs of up
 // to kPackRows bytes.
-constexpr int kPackRows = 512;  // 64 staged runs of up to 512 bytes: 34 KB of shared memory
-constexpr int kPackPitch = kPackRows + 32;  // bytes per staged column (16-byte alignment slack)
+constexpr int kPackRows = 512;                   // rows per tile: 32 lanes x 16 rows
+constexpr int kPackPieces = kPackRows / 16 + 1;  // 16-byte pieces covering a run at any alignment
+constexpr int kPackPitch = kPackPieces * 16;     // bytes per staged run (528)
 
-// logical column-major inputs -> packed rows, for every matrix of the batch:
-// the 64 column runs land in shared memory by aligned 16-byte loads (each run
-// keeps its offset within its first 16 bytes), then thread t builds the
-// words of rows t, t + 256, ... from 64 bytes each (nonzero -> 1).
-__global__ void __launch_bounds__(256) batch_pack_kernel(const BatchDevItem *__restrict__ items,
-                                                         const long long *byte_off,
-                                                         const long long *tile_start,
-                                                         const int *__restrict__ tile_mat,
-                                                         const unsigned char *__restrict__ in, long long total,
-                                                         u64 *__restrict__ out)
+// bit 7 of each byte of x set where that byte is nonzero
+__device__ __forceinline__ u32 byte_nonzero_hi(u32 x)
+{
+    return (((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
+}
+
+// the 16 bytes starting at byte s (0..15) of the 32 bytes p:q
+__device__ __forceinline__ void realign16(const uint4 &p, const uint4 &q, int s, u32 (&x)[4])
+{
+    u32 w0, w1, w2, w3, w4;
+    switch (s >> 2) {
+    case 0: w0 = p.x; w1 = p.y; w2 = p.z; w3 = p.w; w4 = q.x; break;
+    case 1: w0 = p.y; w1 = p.z; w2 = p.w; w3 = q.x; w4 = q.y; break;
+    case 2: w0 = p.z; w1 = p.w; w2 = q.x; w3 = q.y; w4 = q.z; break;
+    default: w0 = p.w; w1 = q.x; w2 = q.y; w3 = q.z; w4 = q.w; break;
+    }
+    const int sh = 8 * (s & 3);
+    x[0] = __funnelshift_r(w0, w1, sh);
+    x[1] = __funnelshift_r(w1, w2, sh);
+    x[2] = __funnelshift_r(w2, w3, sh);
+    x[3] = __funnelshift_r(w3, w4, sh);
+}
+
+// logical column-major inputs -> packed rows, for every matrix of the batch.
+//  1. staging: the 64 column runs land in shared memory by 16-byte cp.async
+//     copies from 16-byte aligned addresses (each run keeps its offset s
+//     within its first piece; pieces past the run are zero-filled);
+//  2. gather: warp o takes columns 8o .. 8o + 7, lane l rows 16l .. 16l + 15:
+//     per column two 16-byte shared reads realigned by s give 16 row bytes,
+//     and for 0/1 bytes one shift-add per 4 bytes puts column c's bit at
+//     bit c % 8 of each row's byte (a lane that saw any other byte value
+//     recomputes with the exact nonzero test);
+//  3. a 4 x 4 byte transpose (byte_perm) turns the 8 octet bytes of a row
+//     into its 64-bit packed word, one store per row.
+__global__ void __launch_bounds__(256, 5) batch_pack_kernel(const BatchDevItem *__restrict__ items,
+                                                            const long long *byte_off,
+                                                            const long long *tile_start,
+                                                            const int *__restrict__ tile_mat,
+                                                            const unsigned char *__restrict__ in,
+                                                            long long total, u64 *__restrict__ out)
 {
     __shared__ __align__(16) unsigned char col[64][kPackPitch];
+    __shared__ __align__(16) u32 oct[8][kPackRows / 4];
     __shared__ int off[64];
     const long long b = blockIdx.x;
     const int lo = tile_mat[b];
@@ -713,64 +745,101 @@ __global__ void __launch_bounds__(256) batch_pack_kernel(const BatchDevItem *__r
     const int rows = (it.m - r0) < kPackRows ? (it.m - r0) : kPackRows;
     const int cols = (it.n - w * 64) < 64 ? (it.n - w * 64) : 64;
     const long long base = byte_off[lo] + (long long)w * 64 * it.m + r0;
-    const int chunks = (rows + 15 + 15) / 16;  // 16-byte pieces covering a run at any alignment
-    {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int c = warp; c < cols; c += 8) {  // a warp per run, a lane per 16 bytes
-            const long long g = base + (long long)c * it.m;
-            if (lane == 0) off[c] = (int)(g & 15);
-            for (int q = lane; q < chunks; q += 32) {
-                const long long a = (g & ~15LL) + 16LL * q;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (a + 16 <= total) {
-                    v = *reinterpret_cast<const uint4 *>(in + a);
-                } else if (a < total) {
-                    unsigned char t[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) t[i] = (a + i < total) ? in[a + i] : 0;
-                    v = *reinterpret_cast<const uint4 *>(t);
-                }
-                *reinterpret_cast<uint4 *>(&col[c][16 * q]) = v;
-            }
-        }
-    }
-    __syncthreads();
-    // warps 0-3 take columns 0-31, warps 4-7 columns 32-63; lane l of warp
-    // w4 = warp & 3 takes rows 128 w4 + 4 l .. + 3 as one 32-bit read per
-    // column (two aligned reads funnel-shifted by the run's offset), folds
-    // each byte to its bit 0 (nonzero) and gathers 8 columns per word: byte k
-    // of that word holds row k's bits for the 8 columns
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int chalf = warp >> 2, w4 = warp & 3;
-    const int rl = 128 * w4 + 4 * lane;  // first of this lane's rows in the tile
-    u32 half[4] = {0, 0, 0, 0};
-    if (rl < rows) {
+    const unsigned long long ib = reinterpret_cast<unsigned long long>(in);
+    // 1. staging: a warp per run (runs warp, warp + 8, ...), lane l piece l
+    //    (lanes 0-7 also piece 32 of runs warp + 8 * lane)
+    auto stage = [&](int c, int q) {
+        const unsigned long long ga = ib + (unsigned long long)(base + (long long)c * it.m);
+        const int s = (int)(ga & 15);
+        const int need = (s + rows + 15) >> 4;
+        const long long a = (long long)(ga & ~15ULL) - (long long)ib + 16LL * q;  // piece offset in the input
+        unsigned char *dst = &col[c][16 * q];
+        if (q < need && a >= 0 && a + 16 <= total) {
+            const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(in + a) : "memory");
+        } else {
+            u32 v[4] = {0u, 0u, 0u, 0u};
+            if (q < need) {
 #pragma unroll
-        for (int ob = 0; ob < 4; ++ob) {
-            u32 oct = 0;
-#pragma unroll
-            for (int cc = 0; cc < 8; ++cc) {
-                const int c = 32 * chalf + 8 * ob + cc;
-                if (c < cols) {
-                    const int o = off[c] + rl;
-                    const u32 *p32 = reinterpret_cast<const u32 *>(&col[c][o & ~3]);
-                    const u32 v = __funnelshift_r(p32[0], p32[1], 8 * (o & 3));
-                    u32 t = v | (v >> 4);
-                    t |= t >> 2;
-                    t |= t >> 1;
-                    oct |= (t & 0x01010101u) << cc;
-                }
+                for (int i = 0; i < 16; ++i)
+                    if (a + i >= 0 && a + i < total) v[i >> 2] |= (u32)in[a + i] << (8 * (i & 3));
             }
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
+        }
+    };
 #pragma unroll
-            for (int k = 0; k < 4; ++k) half[k] |= ((oct >> (8 * k)) & 0xFFu) << (8 * ob);
+    for (int i = 0; i < 8; ++i) {
+        const int c = warp + 8 * i;
+        if (c < cols) stage(c, lane);
+    }
+    if (lane < 8 && warp + 8 * lane < cols) stage(warp + 8 * lane, kPackPieces - 1);
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int c = warp + 8 * i;
+            if (c < cols) off[c] = (int)((ib + (unsigned long long)(base + (long long)c * it.m)) & 15);
         }
     }
-    u32 *out32 = reinterpret_cast<u32 *>(out);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    // 2. gather
+    u32 acc[4] = {0u, 0u, 0u, 0u};
+    u32 bad = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int r = rl + k;
-        if (r < rows && 32 * chalf < cols) out32[2 * (it.in_off + (long long)(r0 + r) * wc + w) + chalf] = half[k];
-        else if (r < rows && chalf == 1) out32[2 * (it.in_off + (long long)(r0 + r) * wc + w) + 1] = 0u;
+    for (int cc = 0; cc < 8; ++cc) {
+        const int c = 8 * warp + cc;
+        if (c < cols) {
+            const uint4 p = *reinterpret_cast<const uint4 *>(&col[c][16 * lane]);
+            const uint4 q = *reinterpret_cast<const uint4 *>(&col[c][16 * lane + 16]);
+            u32 x[4];
+            realign16(p, q, off[c], x);
+            bad |= x[0] | x[1] | x[2] | x[3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[k] += x[k] << cc;
+        }
+    }
+    if (bad & 0xFEFEFEFEu) {  // bytes other than 0 and 1: nonzero -> 1
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] = 0u;
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            const int c = 8 * warp + cc;
+            if (c < cols) {
+                const uint4 p = *reinterpret_cast<const uint4 *>(&col[c][16 * lane]);
+                const uint4 q = *reinterpret_cast<const uint4 *>(&col[c][16 * lane + 16]);
+                u32 x[4];
+                realign16(p, q, off[c], x);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[k] |= byte_nonzero_hi(x[k]) >> (7 - cc);
+            }
+        }
+    }
+    // byte r of oct[o] = row r's bits for columns 8o .. 8o + 7
+    *reinterpret_cast<uint4 *>(&oct[warp][4 * lane]) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+    __syncthreads();
+    // 3. thread t < 128 writes rows 4t .. 4t + 3
+    const int t = threadIdx.x;
+    if (t < kPackRows / 4 && 4 * t < rows) {
+        u32 o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o[i] = oct[i][t];
+        u32 lo4[4], hi4[4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const u32 *v = o + 4 * h;
+            u32 *r = h ? hi4 : lo4;
+            const u32 t0 = __byte_perm(v[0], v[1], 0x5140), t1 = __byte_perm(v[0], v[1], 0x7362);
+            const u32 t2 = __byte_perm(v[2], v[3], 0x5140), t3 = __byte_perm(v[2], v[3], 0x7362);
+            r[0] = __byte_perm(t0, t2, 0x5410);
+            r[1] = __byte_perm(t0, t2, 0x7632);
+            r[2] = __byte_perm(t1, t3, 0x5410);
+            r[3] = __byte_perm(t1, t3, 0x7632);
+        }
+        u64 *dst = out + it.in_off + (long long)(r0 + 4 * t) * wc + w;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (4 * t + k < rows) dst[(long long)k * wc] = ((u64)hi4[k] << 32) | lo4[k];
     }
 }
 
@@ -1137,6 +1206,23 @@ extern "C" mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const ui
         batch_unpack_kernel<<<(unsigned)P->pack_tiles, 256, 0, (cudaStream_t)stream>>>(
             P->d_items, P->d_byte_off, P->d_tile_start, P->d_tile_mat, (const u64 *)d_packed, d_logical);
         MELA_LAUNCH_CHECK("batch_unpack_kernel");
+    }
+    return MELA_OK;
+}
+
+extern "C" mela_status mela_batch_pack_logical(mela_batch_plan *plan, const uint8_t *d_logical,
+                                               uint64_t *d_packed, void *stream)
+{
+    if (!plan || (plan->impl->count && (!d_logical || !d_packed))) {
+        set_error("mela_batch_pack_logical: null argument");
+        return MELA_ERR_INVALID;
+    }
+    BatchPlanImpl *P = plan->impl;
+    if (P->count && P->pack_tiles) {
+        batch_pack_kernel<<<(unsigned)P->pack_tiles, 256, 0, (cudaStream_t)stream>>>(
+            P->d_items, P->d_byte_off, P->d_tile_start, P->d_tile_mat, d_logical, P->logical_total,
+            (u64 *)d_packed);
+        MELA_LAUNCH_CHECK("batch_pack_kernel");
     }
     return MELA_OK;
 }

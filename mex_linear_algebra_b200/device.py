@@ -145,6 +145,13 @@ class BatchPlan:
                                                  1 if use_graph else 0, _stream(stream)))
         return ranks, zt
 
+    def pack_logical(self, d_logical, out=None, stream=None):
+        """All matrices from logical column-major bytes to packed rows (in_offset layout)."""
+        out = torch.zeros(max(self.in_words, 1), dtype=torch.int64, device=d_logical.device) \
+            if out is None else out
+        check(lib().mela_batch_pack_logical(self._plan, _ptr(d_logical), _ptr(out), _stream(stream)))
+        return out
+
     def unpack_logical(self, d_packed, out=None, stream=None):
         """All matrices from packed rows to their logical column-major bytes."""
         out = torch.empty(max(self.logical_bytes, 1), dtype=torch.uint8, device=d_packed.device) \

@@ -85,6 +85,41 @@ def test_logical_input(cuda):
     plan.close()
 
 
+def _logical_bytes(mats, rng=None):
+    """Column-major logical bytes of every matrix; with rng, the nonzero bytes
+    of every other matrix become random values in 1..255."""
+    out = []
+    for i, (m, n, P) in enumerate(mats):
+        L = np.asfortranarray(O.unpack(P, m, n)).ravel(order="F").view(np.uint8).copy()
+        if rng is not None and i % 2:
+            nz = L != 0
+            L[nz] = rng.integers(1, 256, size=int(nz.sum()), dtype=np.uint8)
+        out.append(L)
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("shift", [0, 3, 13])
+@pytest.mark.parametrize("dirty", [False, True])
+def test_pack_logical_exact(cuda, shift, dirty):
+    """The batched packing equals the oracle's packing word for word, from a
+    base pointer at any alignment, with nonzero bytes other than 1 read as 1."""
+    import torch
+    from mex_linear_algebra_b200 import device as D
+    shapes = [(1, 1), (7, 200), (16, 64), (17, 63), (511, 65), (512, 128), (513, 130),
+              (1000, 700), (1025, 64), (3, 1), (200, 9)]
+    mats = [(m, n, O.rand_dense(31, i, m, n)) for i, (m, n) in enumerate(shapes)] + ldpc_mats(5, seed=9)
+    plan = D.BatchPlan([(m, n) for (m, n, _) in mats])
+    host = _logical_bytes(mats, np.random.default_rng(shift) if dirty else None)
+    buf = torch.zeros(shift + host.size, dtype=torch.uint8, device="cuda")
+    buf[shift:] = torch.from_numpy(host).cuda()
+    got = plan.pack_logical(buf[shift:])
+    want = _pack_buffer(plan, mats)
+    assert torch.equal(got, want)
+    ranks, zt = plan.run_logical(buf[shift:])
+    _check(plan, ranks, zt, mats)
+    plan.close()
+
+
 def test_large_batch_ranks(cuda):
     """2000 parity-check matrices: ranks equal the per-matrix oracle on a sample."""
     from mex_linear_algebra_b200 import device as D, gen
