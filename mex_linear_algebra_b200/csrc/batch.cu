@@ -267,19 +267,41 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 
 // 32x32 bit transposes by warp shuffles over a CTA: dst (cols x rows bits,
 // 32-bit words, pitch dld) = src^T, where src row r, 32-bit word x is
-// srcw(r, x) (rows x cols bits).
+// srcw(r, x) (rows x cols bits).  A warp takes kTrUnroll consecutive tiles
+// at a time and reads all their source words before the first shuffle, so
+// that the (often L2-resident, index-dependent) reads overlap; dst must not
+// overlap what srcw reads.
+constexpr int kTrUnroll = 4;
 template <typename F>
 __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dld)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5;
-    for (long long t = warp; t < (long long)rt * ct; t += kBigWarps) {
-        const int tr = (int)(t / ct), tc = (int)(t - (long long)tr * ct);
-        const int r = tr * 32 + lane;
-        // lane l gets column tc*32 + l, bit b = row tr*32 + b
-        const u32 keep = transpose32_warp(r < rows ? srcw(r, tc) : 0u);
-        const int c = tc * 32 + lane;
-        if (c < cols) dst[(long long)c * dld + tr] = keep;
+    const long long total = (long long)rt * ct;
+    for (long long t0 = (long long)warp * kTrUnroll; t0 < total; t0 += (long long)kBigWarps * kTrUnroll) {
+        const int tr0 = (int)(t0 / ct), tc0 = (int)(t0 - (long long)tr0 * ct);
+        int tr[kTrUnroll], tc[kTrUnroll];
+        u32 v[kTrUnroll];
+#pragma unroll
+        for (int u = 0; u < kTrUnroll; ++u) {
+            // tile t0 + u, stepping along the tile row
+            tc[u] = tc0 + u;
+            tr[u] = tr0;
+            while (tc[u] >= ct) {
+                tc[u] -= ct;
+                ++tr[u];
+            }
+            const int r = tr[u] * 32 + lane;
+            v[u] = (t0 + u < total && r < rows) ? srcw(r, tc[u]) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kTrUnroll; ++u) {
+            if (t0 + u >= total) break;  // warp-uniform
+            // lane l gets column tc*32 + l, bit b = row tr*32 + b
+            const u32 keep = transpose32_warp(v[u]);
+            const int c = tc[u] * 32 + lane;
+            if (c < cols) dst[(long long)c * dld + tr[u]] = keep;
+        }
     }
 }
 
