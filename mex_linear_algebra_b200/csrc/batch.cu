@@ -7,12 +7,15 @@
 //   class  group            storage of the matrix
 //   small  one warp         its slice of shared memory (13 KB)
 //   mid    128 threads      its slice of shared memory (55 KB)
-//   big    the whole CTA    shared memory (up to ~220 KB) or, when it does
-//          (512 threads)    not fit, the CTA's L2-resident global scratch
+//   big    the whole CTA    shared memory (up to ~110 KB) or, when it does
+//          (256 threads)    not fit, the CTA's L2-resident global scratch
+//
+// (two CTAs per SM; the single-matrix fused mode runs the same engines in
+// one CTA of 512 threads with 220 KB)
 //
 // The host sorts the matrices into the three classes (largest first inside
-// each class); every CTA drains the big queue, then the mid queue (4 groups),
-// then the small queue (16 warps), taking the next matrix with an atomic on
+// each class); every CTA drains the big queue, then the mid queue (2 groups),
+// then the small queue (8 warps), taking the next matrix with an atomic on
 // the class counter.  A group eliminates column by column: the rows are
 // dealt round-robin to its threads; per column each thread looks for the
 // first active row of its own holding the bit, a warp min (+ shared atomic
@@ -54,6 +57,11 @@ constexpr int kMidGroup = 128;
 constexpr int kSmemTotal = 220 * 1024;
 constexpr int kMidBudget = kSmemTotal / (kThreads / kMidGroup);  // 55 KB
 constexpr int kSmallBudget = kSmemTotal / (kThreads / 32);       // 13.75 KB
+// the batch launch: two CTAs of 256 threads per SM, each with half the
+// shared memory, so that one CTA's barrier-bound panel steps overlap the
+// other's table updates and transposes
+constexpr int kBatchThreads = 256;
+constexpr int kBatchSmem = kSmemTotal / (kThreads / kBatchThreads);
 
 __host__ __device__ inline size_t al8(size_t x) { return (x + 7) & ~(size_t)7; }
 
@@ -235,27 +243,37 @@ __host__ __device__ inline long long big_scratch_words(long long m, long long n)
 }
 
 namespace {
-constexpr int kBigWarps = kThreads / 32;
-constexpr int kTW = 32;  // words per update chunk (one per lane)
 constexpr int kRegThreads = 256;  // threads holding a panel in registers (m <= 1024)
 constexpr int kRegRows = 4;        // rows per thread there
 constexpr int kRegWarps = kRegThreads / 32;
 static_assert(kRegWarps == 8, "eight candidate slots");
 constexpr int kRegBar = 6;         // their named barrier
+template <int TW>
 struct BigSmem {
     u64 coef[64];
     u64 pub[2][kRegWarps][2];  // per warp: its candidate pivot's panel word and tag (by bit parity)
     alignas(16) unsigned wmin[2][kRegWarps];  // per warp: its candidate pivot row
     int bits[64], srow[64];
     int slots[4];
-    u64 T[16][16][kTW];  // nibble tables of the current chunk
+    u64 T[16][16][TW];  // nibble tables of the current chunk (TW words)
     u64 pm;
     int p;
 };
-// Shared memory after BigSmem: panel stage + reduced rows, then the per-row
-// panel words (snapshot, working copy, combination tags), when they fit.
-constexpr size_t kBigExtra = (size_t)kSmemTotal - ((sizeof(BigSmem) + 15) & ~(size_t)15);
-static_assert(sizeof(BigSmem) <= (size_t)kSmemTotal, "big-matrix shared memory");
+// The big-matrix engine for a CTA of NT threads with SMEM bytes of shared
+// memory: TW words per update chunk (32, one per lane, for 512 threads; 16,
+// two rows per warp instruction, for 256 threads, which halves the tables);
+// after BigSmem, kExtra bytes hold the panel stage + reduced rows, then the
+// per-row panel words (snapshot, working copy, combination tags) and the
+// matrix itself, each when it fits.
+template <int NT, int SMEM>
+struct BigCfg {
+    static constexpr int TW = NT >= 512 ? 32 : 16;
+    using Smem = BigSmem<TW>;
+    static constexpr size_t kHead = (sizeof(Smem) + 15) & ~(size_t)15;
+    static constexpr size_t kExtra = (size_t)SMEM - kHead;
+    static_assert(sizeof(Smem) <= (size_t)SMEM, "big-matrix shared memory");
+    static_assert(NT >= kRegThreads, "the register panel needs 256 threads");
+};
 }  // namespace
 
 // Element i (0..3, per thread) of a register array, by a select tree.
@@ -272,13 +290,14 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 // that the (often L2-resident, index-dependent) reads overlap; dst must not
 // overlap what srcw reads.
 constexpr int kTrUnroll = 4;
-template <typename F>
+template <int NT, typename F>
 __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dld)
 {
+    constexpr int kWarps = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5;
     const long long total = (long long)rt * ct;
-    for (long long t0 = (long long)warp * kTrUnroll; t0 < total; t0 += (long long)kBigWarps * kTrUnroll) {
+    for (long long t0 = (long long)warp * kTrUnroll; t0 < total; t0 += (long long)kWarps * kTrUnroll) {
         const int tr0 = (int)(t0 / ct), tc0 = (int)(t0 - (long long)tr0 * ct);
         int tr[kTrUnroll], tc[kTrUnroll];
         u32 v[kTrUnroll];
@@ -319,11 +338,16 @@ __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dl
 //  * null basis: Zt = (Y)^T with Y row c = (R restricted to free columns)^T
 //    row p when c is pivot column p, the unit vector of its free index
 //    otherwise -- three 32x32 shuffle transposes, no per-bit gathers.
+template <int NT, int SMEM>
 __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restrict__ in,
                                     u64 *__restrict__ zt, long long *ranks, int item,
                                     unsigned char *smem_raw, u64 *g, const FusedOut *fo = nullptr)
 {
-    BigSmem &S = *reinterpret_cast<BigSmem *>(smem_raw);
+    using Cfg = BigCfg<NT, SMEM>;
+    constexpr int TW = Cfg::TW;
+    constexpr size_t kBigExtra = Cfg::kExtra;
+    constexpr int kWarps = NT / 32;
+    typename Cfg::Smem &S = *reinterpret_cast<typename Cfg::Smem *>(smem_raw);
     const int m = it.m, n = it.n, wc = (n + 63) >> 6, mn = m < n ? m : n;
     const int tid = threadIdx.x, lane = tid & 31;
     const BigLayout L = big_layout(m, n);
@@ -337,7 +361,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u32 *Rt = reinterpret_cast<u32 *>(g + L.rt);
     u32 *Q = reinterpret_cast<u32 *>(g + L.q);
 
-    unsigned char *extra = smem_raw + ((sizeof(BigSmem) + 15) & ~(size_t)15);
+    unsigned char *extra = smem_raw + Cfg::kHead;
     const size_t rb_bytes = (size_t)64 * wc * 8, row_bytes = (size_t)m * 8;
     const bool r_in_smem = 2 * rb_bytes <= kBigExtra;
     u64 *stage = r_in_smem ? reinterpret_cast<u64 *>(extra) : g + L.Rg;
@@ -353,13 +377,14 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u64 *yv = rows_in_smem ? ysnap + m : g + L.yvg;
     u64 *tag = rows_in_smem ? yv + m : g + L.tagg;
     if (rows_in_smem) used += 3 * row_bytes;
-    // the matrix itself in shared memory too when it fits (m up to about 650
-    // at n = 2m), else in the CTA's L2-resident scratch
+    // the matrix itself in shared memory too when it fits (at n = 2m: m up
+    // to about 420 with 110 KB, 650 with 220 KB), else in the CTA's
+    // L2-resident scratch
     if (used + (size_t)m * wc * 8 <= kBigExtra) A = reinterpret_cast<u64 *>(extra + used);
 
     const u64 *src = in + it.in_off;
-    for (long long e = tid; e < (long long)m * wc; e += kThreads) A[e] = src[e];
-    for (int j = tid; j < m; j += kThreads) active[j] = 1;
+    for (long long e = tid; e < (long long)m * wc; e += NT) A[e] = src[e];
+    for (int j = tid; j < m; j += NT) active[j] = 1;
     __syncthreads();
 
     int r = 0;
@@ -371,7 +396,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             // holds rows l + 256 i.  Per bit one named barrier: each warp
             // publishes its lowest unused row holding the bit (index, panel
             // word and tag); the lowest of the eight is the pivot.
-            for (int j = tid; j < m; j += kThreads) ysnap[j] = A[(size_t)j * wc + w];
+            for (int j = tid; j < m; j += NT) ysnap[j] = A[(size_t)j * wc + w];
             __syncthreads();
             if (tid < kRegThreads) {
                 const int warp = tid >> 5;
@@ -440,14 +465,14 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             __syncthreads();
             k = S.p;
             pmask = S.pm;
-            for (int q = tid; q < k; q += kThreads) active[S.srow[q]] = 2;
+            for (int q = tid; q < k; q += NT) active[S.srow[q]] = 2;
             __syncthreads();
         } else {
             // 1. panel words, pivot search for bit 0
             if (tid < 3) S.slots[tid] = INT_MAX;
             __syncthreads();
             unsigned best = INT_MAX;
-            for (int j = tid; j < m; j += kThreads) {
+            for (int j = tid; j < m; j += NT) {
                 const u64 word = A[(size_t)j * wc + w];
                 ysnap[j] = word;
                 const u64 y = active[j] == 1 ? word : 0ull;
@@ -468,9 +493,9 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                         S.bits[k] = b;
                         S.srow[k] = p;
                     }
-                    if (p % kThreads == tid) active[p] = 2;
+                    if (p % NT == tid) active[p] = 2;
                     const u64 bit = 1ull << b;
-                    for (int j = tid; j < m; j += kThreads) {
+                    for (int j = tid; j < m; j += NT) {
                         if (j == p || active[j] == 0) continue;
                         if (yv[j] & bit) {
                             yv[j] ^= yp;
@@ -483,7 +508,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                 if (b < 63) {
                     const u64 bit = 1ull << (b + 1);
                     best = INT_MAX;
-                    for (int j = tid; j < m; j += kThreads)
+                    for (int j = tid; j < m; j += NT)
                         if (active[j] == 1 && (yv[j] & bit)) {
                             best = j;
                             break;
@@ -496,7 +521,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         }
         const int p = k;
         if (p == 0) continue;
-        for (int t = tid; t < p; t += kThreads) {
+        for (int t = tid; t < p; t += NT) {
             S.coef[t] = tag[S.srow[t]] ^ (1ull << t);
             piv[r + t] = 64 * w + S.bits[t];
             prow[r + t] = S.srow[t];
@@ -504,12 +529,12 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         const int rem = wc - w;
         // 3. reduced pivot rows from the staged original rows
         __syncthreads();
-        for (int e = tid; e < p * rem; e += kThreads) {
+        for (int e = tid; e < p * rem; e += NT) {
             const int i = e / rem, x = w + e % rem;
             stage[(size_t)i * wc + x] = A[(size_t)S.srow[i] * wc + x];
         }
         __syncthreads();
-        for (int e = tid; e < p * rem; e += kThreads) {
+        for (int e = tid; e < p * rem; e += NT) {
             const int kk = e / rem, x = w + e % rem;
             u64 c = S.coef[kk], v = 0;
             while (c) {
@@ -522,9 +547,9 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         }
         __syncthreads();
         // 4. update every other row, 32 words at a time
-        for (int x0 = w; x0 < wc; x0 += kTW) {
-            for (int e = tid; e < 16 * 5 * kTW; e += kThreads) {
-                const int t = e % kTW, gh = e / kTW, gi = gh / 5, h = gh % 5;
+        for (int x0 = w; x0 < wc; x0 += TW) {
+            for (int e = tid; e < 16 * 5 * TW; e += NT) {
+                const int t = e % TW, gh = e / TW, gi = gh / 5, h = gh % 5;
                 if (h == 4) {
                     S.T[gi][0][t] = 0;
                     continue;
@@ -540,20 +565,25 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             __syncthreads();
             for (int h = 1; h < 4; ++h) {
                 const int cnt = (1 << h) - 1;
-                for (int e = tid; e < 16 * cnt * kTW; e += kThreads) {
-                    const int t = e % kTW, rest = e / kTW, gi = rest / cnt, v = (1 << h) + 1 + rest % cnt;
+                for (int e = tid; e < 16 * cnt * TW; e += NT) {
+                    const int t = e % TW, rest = e / TW, gi = rest / cnt, v = (1 << h) + 1 + rest % cnt;
                     S.T[gi][v][t] = S.T[gi][v - (1 << h)][t] ^ S.T[gi][1 << h][t];
                 }
                 __syncthreads();
             }
-            const int x = x0 + lane;
+            // lane (h, xl) = (lane / TW, lane % TW) takes word x0 + xl of
+            // rows j0 + 4 h .. + 3 (32 / TW rows per warp instruction)
+            constexpr int RPW = 32 / TW;
+            const int xl = lane % TW, hsel = lane / TW;
+            const int x = x0 + xl;
             const int warp = tid >> 5;
-            for (int j0 = warp * 4; j0 < m; j0 += kBigWarps * 4) {
+            for (int j0 = warp * 4 * RPW; j0 < m; j0 += kWarps * 4 * RPW) {
                 u64 y[4], a[4];
                 bool go[4];
+                const int jb = j0 + 4 * hsel;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int j = j0 + q;
+                    const int j = jb + q;
                     go[q] = false;
                     y[q] = 0;
                     if (j < m && active[j] != 2) {
@@ -563,28 +593,28 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    if (go[q]) a[q] = A[(size_t)(j0 + q) * wc + x];
+                    if (go[q]) a[q] = A[(size_t)(jb + q) * wc + x];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (!go[q]) continue;
                     u64 acc = 0;
 #pragma unroll
-                    for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][lane];
-                    A[(size_t)(j0 + q) * wc + x] = a[q] ^ acc;
+                    for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][xl];
+                    A[(size_t)(jb + q) * wc + x] = a[q] ^ acc;
                 }
             }
             __syncthreads();
         }
-        for (int t = tid; t < p; t += kThreads) active[S.srow[t]] = 0;
+        for (int t = tid; t < p; t += NT) active[S.srow[t]] = 0;
         r += p;
         __syncthreads();
     }
     if (fo) {
-        for (long long e = tid; e < (long long)m * wc; e += kThreads) {
+        for (long long e = tid; e < (long long)m * wc; e += NT) {
             const int rr = (int)(e / wc), x = (int)(e - (long long)rr * wc);
             fo->M[(long long)rr * fo->ldm + x] = A[e];
         }
-        for (int t = tid; t < r; t += kThreads) {
+        for (int t = tid; t < r; t += NT) {
             fo->piv[t] = piv[t];
             fo->prow[t] = prow[t];
         }
@@ -596,10 +626,10 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
 
     // ---- null basis
     const int f = n - r;
-    for (int W = tid; W < wc; W += kThreads) pm[W] = 0;
-    for (int c = tid; c < n; c += kThreads) cmap[c] = -1;
+    for (int W = tid; W < wc; W += NT) pm[W] = 0;
+    for (int c = tid; c < n; c += NT) cmap[c] = -1;
     __syncthreads();
-    for (int t = tid; t < r; t += kThreads) {
+    for (int t = tid; t < r; t += NT) {
         atomicOr(&pm[piv[t] >> 6], 1ull << (piv[t] & 63));
         cmap[piv[t]] = t;
     }
@@ -614,7 +644,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     }
     __syncthreads();
     // free columns: word W's free bits go to ranks [64W - pbase[W], ...)
-    for (int W = tid; W < wc; W += kThreads) {
+    for (int W = tid; W < wc; W += NT) {
         const int valid = n - 64 * W;
         const u64 vm = valid >= 64 ? ~0ull : ((1ull << valid) - 1);
         u64 fm = ~pm[W] & vm;
@@ -632,12 +662,12 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     const int rt32 = (r + 31) >> 5, q32 = (f + 31) >> 5;
     if (r > 0) {
         // Rt (n x r) = R^T, R row p = A[prow[p]]
-        cta_transpose([&](int row, int x) -> u32 {
+        cta_transpose<NT>([&](int row, int x) -> u32 {
             return reinterpret_cast<const u32 *>(A + (size_t)prow[row] * wc)[x];
         }, r, n, Rt, rt32);
         __syncthreads();
         // Q (r x f) = (rows f_i of Rt)^T: row p = RREF row p at the free columns
-        cta_transpose([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
+        cta_transpose<NT>([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
                       f, r, Q, q32);
         __syncthreads();
     }
@@ -645,8 +675,8 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u64 *Z = zt + it.z_off;
     u32 *Z32 = reinterpret_cast<u32 *>(Z);
     if ((n & 63) && (n & 63) <= 32)
-        for (int i = tid; i < f; i += kThreads) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
-    cta_transpose([&](int c, int y) -> u32 {
+        for (int i = tid; i < f; i += NT) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
+    cta_transpose<NT>([&](int c, int y) -> u32 {
         const int mc = cmap[c];
         if (mc >= 0) return Q[(long long)mc * q32 + y];
         const int fi = -mc - 1;
@@ -655,13 +685,19 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+// NT threads and SMEM bytes of shared memory per CTA, kThreads / NT CTAs per
+// SM: a big matrix takes a whole CTA, a medium one a 128-thread group with
+// kMidBudget bytes, a small one a warp with kSmallBudget bytes.
+template <int NT, int SMEM>
+__global__ void __launch_bounds__(NT, kThreads / NT)
 batch_kernel(const BatchDevItem *__restrict__ items, const int *__restrict__ order, int n_big,
              int n_mid, int n_small, int *counters, const u64 *__restrict__ in, u64 *__restrict__ zt,
              long long *ranks, u64 *gscratch, long long gscratch_words)
 {
+    static_assert((NT / kMidGroup) * kMidBudget <= SMEM && (NT / 32) * kSmallBudget <= SMEM,
+                  "group regions");
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_next[kThreads / 32];
+    __shared__ int s_next[NT / 32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     u64 *gmat = gscratch + (long long)blockIdx.x * gscratch_words;
 
@@ -673,9 +709,9 @@ batch_kernel(const BatchDevItem *__restrict__ items, const int *__restrict__ ord
         __syncthreads();
         if (k >= n_big) break;
         const int item = order[k];
-        process_big_blocked(items[item], in, zt, ranks, item, smem, gmat);
+        process_big_blocked<NT, SMEM>(items[item], in, zt, ranks, item, smem, gmat);
     }
-    // mid: four groups of 128 threads, each with a quarter of shared memory
+    // mid: groups of 128 threads, each with kMidBudget bytes of shared memory
     {
         const int g = tid / kMidGroup, gtid = tid % kMidGroup;
         unsigned char *region = smem + (size_t)g * kMidBudget;
@@ -902,7 +938,7 @@ fused_elim_kernel(BatchDevItem it, const u64 *__restrict__ in_compact, FusedOut 
     if (it.flags & 1)
         process_matrix<kThreads>(it, in_compact, nullptr, nullptr, 0, smem, nullptr, threadIdx.x, 0, &fo);
     else
-        process_big_blocked(it, in_compact, nullptr, nullptr, 0, smem, scratch, &fo);
+        process_big_blocked<kThreads, kSmemTotal>(it, in_compact, nullptr, nullptr, 0, smem, scratch, &fo);
 }
 
 size_t fused_workspace(i64 m, i64 n)
@@ -1045,7 +1081,7 @@ static mela_status plan_create(const mela_batch_item *h, long long count, int fo
     P->n_big = (int)P->class_count[0];
     P->n_mid = (int)P->class_count[1];
     P->n_small = (int)P->class_count[2];
-    P->grid = sm_count();
+    P->grid = (kThreads / kBatchThreads) * sm_count();
     P->gscratch_words = max_big_words;
 
     // logical-input packing tiles
@@ -1100,9 +1136,9 @@ static mela_status enqueue(BatchPlanImpl *P, const u64 *in, u64 *zt, long long *
 {
     MELA_CUDA_TRY(cudaMemsetAsync(P->d_counters, 0, 4 * sizeof(int), s));
     if (P->count == 0) return MELA_OK;
-    batch_kernel<<<P->grid, kThreads, kSmemTotal, s>>>(P->d_items, P->d_order, P->n_big, P->n_mid,
-                                                       P->n_small, P->d_counters, in, zt, ranks,
-                                                       P->d_gscratch, P->gscratch_words);
+    batch_kernel<kBatchThreads, kBatchSmem><<<P->grid, kBatchThreads, kBatchSmem, s>>>(
+        P->d_items, P->d_order, P->n_big, P->n_mid, P->n_small, P->d_counters, in, zt, ranks,
+        P->d_gscratch, P->gscratch_words);
     MELA_LAUNCH_CHECK("batch_kernel");
     return MELA_OK;
 }
@@ -1124,8 +1160,8 @@ static mela_status run(BatchPlanImpl *P, const void *in, int logical, u64 *zt, l
 {
     static bool attr = false;
     if (!attr) {
-        MELA_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemTotal));
+        MELA_CUDA_TRY(cudaFuncSetAttribute(batch_kernel<kBatchThreads, kBatchSmem>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBatchSmem));
         attr = true;
     }
     if (logical && !P->d_packed) {
