@@ -1155,14 +1155,26 @@ static mela_status enqueue_logical(BatchPlanImpl *P, const unsigned char *in, u6
     return enqueue(P, P->d_packed, zt, ranks, s);
 }
 
+// Dynamic shared memory limit of the batch kernel, once per device (and
+// before any stream capture).
+static mela_status batch_attrs()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    MELA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || done[dev]) return MELA_OK;
+    MELA_CUDA_TRY(cudaFuncSetAttribute(batch_kernel<kBatchThreads, kBatchSmem>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kBatchSmem));
+    done[dev] = true;
+    return MELA_OK;
+}
+
 static mela_status run(BatchPlanImpl *P, const void *in, int logical, u64 *zt, long long *ranks,
                        cudaStream_t s, int use_graph)
 {
-    static bool attr = false;
-    if (!attr) {
-        MELA_CUDA_TRY(cudaFuncSetAttribute(batch_kernel<kBatchThreads, kBatchSmem>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kBatchSmem));
-        attr = true;
+    {
+        const mela_status st = batch_attrs();
+        if (st != MELA_OK) return st;
     }
     if (logical && !P->d_packed) {
         cudaError_t e = cudaMalloc((void **)&P->d_packed, (size_t)(P->packed_words ? P->packed_words : 1) * 8);

@@ -120,6 +120,26 @@ def test_pack_logical_exact(cuda, shift, dirty):
     plan.close()
 
 
+@pytest.mark.parametrize("logical", [False, True])
+def test_empty_matrices_in_batch(cuda, logical):
+    """0 x n, m x 0 and 0 x 0 items beside ordinary ones: rank 0, null basis
+    I_n for m = 0, nothing for n = 0, and the other items unaffected."""
+    import torch
+    from mex_linear_algebra_b200 import device as D
+    shapes = [(0, 5), (33, 70), (7, 0), (0, 0), (0, 70), (300, 640), (1, 0), (0, 1), (64, 64)]
+    mats = [(m, n, O.rand_dense(41, i, m, n)) for i, (m, n) in enumerate(shapes)]
+    plan = D.BatchPlan([(m, n) for (m, n, _) in mats])
+    if logical:
+        host = _logical_bytes(mats)
+        d_log = torch.from_numpy(host).cuda() if host.size else torch.zeros(1, dtype=torch.uint8, device="cuda")
+        assert torch.equal(plan.pack_logical(d_log), _pack_buffer(plan, mats))
+        ranks, zt = plan.run_logical(d_log)
+    else:
+        ranks, zt = plan.run(_pack_buffer(plan, mats))
+    _check(plan, ranks, zt, mats)
+    plan.close()
+
+
 def test_large_batch_ranks(cuda):
     """2000 parity-check matrices: ranks equal the per-matrix oracle on a sample."""
     from mex_linear_algebra_b200 import device as D, gen
