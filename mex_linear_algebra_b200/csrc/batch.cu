@@ -289,7 +289,7 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 // at a time and reads all their source words before the first shuffle, so
 // that the (often L2-resident, index-dependent) reads overlap; dst must not
 // overlap what srcw reads.
-constexpr int kTrUnroll = 4;
+constexpr int kTrUnroll = 8;
 template <int NT, typename F>
 __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dld)
 {
