@@ -61,6 +61,8 @@ constexpr int kSmallBudget = kSmemTotal / (kThreads / 32);       // 13.75 KB
 // shared memory, so that one CTA's barrier-bound panel steps overlap the
 // other's table updates and transposes
 constexpr int kBatchThreads = 256;
+constexpr int kSmallMaxRows = 160;  // largest m for the warp engine
+constexpr int kMidMaxRows = 240;    // the 128-thread engine below this m
 constexpr int kBatchSmem = kSmemTotal / (kThreads / kBatchThreads);
 
 __host__ __device__ inline size_t al8(size_t x) { return (x + 7) & ~(size_t)7; }
@@ -1052,9 +1054,13 @@ static mela_status plan_create(const mela_batch_item *h, long long count, int fo
         d.z_off = h[i].z_offset;
         const size_t aux = aux_bytes((int)m, (int)n);
         const size_t mat = (size_t)m * smem_ld((int)n) * 8;
+        // Class by fit and size: with two CTAs per SM the blocked CTA engine
+        // beats the 128-thread column engine from m = 240 up (parity-check
+        // matrices, n = 2m: 7% faster at m in [230, 300), 23% at [380, 460)),
+        // and the column engine beats a warp from m = 160 up.
         int c;
-        if (aux + mat <= (size_t)kSmallBudget && m <= 256) c = 2;
-        else if (aux + mat <= (size_t)kMidBudget) c = 1;
+        if (aux + mat <= (size_t)kSmallBudget && m <= kSmallMaxRows) c = 2;
+        else if (aux + mat <= (size_t)kMidBudget && m < kMidMaxRows) c = 1;
         else c = 0;
         if (force_class >= 0 && force_class <= 2) {
             // a forced class must still fit its region; otherwise fall back to big
