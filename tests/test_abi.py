@@ -69,6 +69,27 @@ def test_dev_entry_points_reject_bad_shapes():
     assert L.mela_dev_transpose(None, 0, 2, 70, None, 1, None) == _lib.ERR_INVALID
 
 
+def test_batch_entry_points_reject_bad_arguments():
+    """Null plans and buffers, negative shapes or offsets and a bad item list
+    are refused before any device work."""
+    from mex_linear_algebra_b200 import _lib
+    L = _lib.lib()
+    for fn in ("mela_batch_rank_null", "mela_batch_rank_null_logical"):
+        assert getattr(L, fn)(None, None, None, None, 1, None) == _lib.ERR_INVALID
+    for fn in ("mela_batch_pack_logical", "mela_batch_unpack_logical"):
+        assert getattr(L, fn)(None, None, None, None) == _lib.ERR_INVALID
+    plan = C.c_void_p()
+    items = (_lib.BatchItem * 2)(_lib.BatchItem(3, 5, 0, 0), _lib.BatchItem(-1, 5, 1, 5))
+    assert L.mela_batch_plan_create(items, 2, -1, C.byref(plan)) == _lib.ERR_INVALID
+    assert b"item 1 has a bad shape or offset" in L.mela_last_error()
+    assert not plan.value
+    items = (_lib.BatchItem * 1)(_lib.BatchItem(3, 5, -8, 0))
+    assert L.mela_batch_plan_create(items, 1, -1, C.byref(plan)) == _lib.ERR_INVALID
+    assert L.mela_batch_plan_create(None, 4, -1, C.byref(plan)) == _lib.ERR_INVALID
+    assert L.mela_batch_plan_create(items, -1, -1, C.byref(plan)) == _lib.ERR_INVALID
+    assert L.mela_batch_plan_create(items, 1, -1, None) == _lib.ERR_INVALID
+
+
 def test_workspace_sizes():
     from mex_linear_algebra_b200 import _lib
     L = _lib.lib()
