@@ -168,7 +168,8 @@ def run_reference(args, ws, rank):
         "vs_baseline": None,
         "dtype": "u64",
         "data": "synthetic (seeded splitmix64 Bernoulli(1/2))",
-        "config": {"workload": "gemm_gf2_32768^3_sample", "m": ms, "k": ks, "n": ns},
+        "config": {"workload": "gemm_gf2_32768^3", "m": 32768, "k": 32768, "n": 32768, "seed": SEED,
+                   "sample_per_step": {"m": ms, "k": ks, "n": ns}},
         "cpu_baseline": {"value": round(rate, 4), "unit": "Tbitop/s", "cores": threads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": round(rate, 4), "unit": "Tbitop/s", "h2d_bytes_per_step": 0,
@@ -583,7 +584,8 @@ def run_mela(args, ws, rank, local):
             "vs_baseline": None,
             "dtype": "u8",
             "data": "synthetic (seeded splitmix64 Bernoulli(1/2), generated on device)",
-            "config": {"workload": "gemm_gf2_32768^3_tensor_core", "m": M, "k": K, "n": N,
+            "config": {"workload": f"gemm_gf2_{M}^3" if M == K == N else f"gemm_gf2_{M}x{K}x{N}",
+                       "m": M, "k": K, "n": N,
                        "variant": {"tc": "tc (tcgen05 kind::i8)",
                                    "tc_fp4": "tc_fp4 (tcgen05 kind::mxf4, e2m1 0/1, unit scales)"}[args.variant],
                        "seed": SEED,
