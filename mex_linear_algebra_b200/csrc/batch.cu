@@ -785,15 +785,15 @@ __device__ __forceinline__ void realign16(const uint4 &p, const uint4 &q, int s,
 //     recomputes with the exact nonzero test);
 //  3. a 4 x 4 byte transpose (byte_perm) turns the 8 octet bytes of a row
 //     into its 64-bit packed word, one store per row.
-__global__ void __launch_bounds__(256, 5) batch_pack_kernel(const BatchDevItem *__restrict__ items,
+__global__ void __launch_bounds__(256, 6) batch_pack_kernel(const BatchDevItem *__restrict__ items,
                                                             const long long *byte_off,
                                                             const long long *tile_start,
                                                             const int *__restrict__ tile_mat,
                                                             const unsigned char *__restrict__ in,
                                                             long long total, u64 *__restrict__ out)
 {
+    // 34 KB, so that six CTAs share an SM
     __shared__ __align__(16) unsigned char col[64][kPackPitch];
-    __shared__ __align__(16) u32 oct[8][kPackRows / 4];
     __shared__ int off[64];
     const long long b = blockIdx.x;
     const int lo = tile_mat[b];
@@ -875,15 +875,17 @@ __global__ void __launch_bounds__(256, 5) batch_pack_kernel(const BatchDevItem *
             }
         }
     }
-    // byte r of oct[o] = row r's bits for columns 8o .. 8o + 7
-    *reinterpret_cast<uint4 *>(&oct[warp][4 * lane]) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+    // byte r of oct(o) = row r's bits for columns 8o .. 8o + 7; warp o has
+    // read only its own runs 8o .. 8o + 7, so oct(o) overwrites run 8o
+    __syncwarp();
+    *reinterpret_cast<uint4 *>(&col[8 * warp][16 * lane]) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
     __syncthreads();
     // 3. thread t < 128 writes rows 4t .. 4t + 3
     const int t = threadIdx.x;
     if (t < kPackRows / 4 && 4 * t < rows) {
         u32 o[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) o[i] = oct[i][t];
+        for (int i = 0; i < 8; ++i) o[i] = reinterpret_cast<const u32 *>(col[8 * i])[t];
         u32 lo4[4], hi4[4];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
