@@ -264,6 +264,17 @@ mela_status mela_dev_null_basis(const uint64_t *dR, int64_t ld, int64_t m, int64
                                 int64_t rank, const int64_t *d_pivcols, const int64_t *d_pivrows,
                                 uint64_t *dZt, int64_t ldz, void *workspace,
                                 size_t workspace_bytes, void *stream);
+/* On-device check of a null-space basis: *d_bad_rows (device) = the number
+ * of rows i of A (m x n, packed) with A_i . z != 0 for some basis vector z,
+ * where Zt holds the f basis vectors as packed rows of n bits (the layout of
+ * mela_dev_null_basis); 0 means A Z = 0.  Bits past column n of A and Zt
+ * must be zero (the packed convention).  Workspace:
+ * mela_null_verify_workspace_size(m, f) bytes.  No reference counterpart
+ * (the reference's tests check A Z = 0 on the host). */
+size_t mela_null_verify_workspace_size(int64_t m, int64_t f);
+mela_status mela_dev_null_verify(const uint64_t *dA, int64_t lda, int64_t m, int64_t n,
+                                 const uint64_t *dZt, int64_t ldz, int64_t f, int64_t *d_bad_rows,
+                                 void *workspace, size_t workspace_bytes, void *stream);
 /* Packed rows -> row-major bytes (rows x n). */
 mela_status mela_dev_unpack_rows(const uint64_t *d_in, int64_t ld, int64_t rows, int64_t n,
                                  uint8_t *d_out, void *stream);

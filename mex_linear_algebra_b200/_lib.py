@@ -91,6 +91,8 @@ SIGNATURES = {
     "mela_dev_rref": (_st, [_i32, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
     "mela_null_workspace_size": (_sz, [_i64, _i64]),
     "mela_dev_null_basis": (_st, [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _sz, _vp]),
+    "mela_null_verify_workspace_size": (C.c_size_t, [_i64, _i64]),
+    "mela_dev_null_verify": (_st, [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _vp, C.c_size_t, _vp]),
     "mela_dev_unpack_rows": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
     "mela_batch_plan_create": (_st, [C.POINTER(BatchItem), _i64, _i32, C.POINTER(_vp)]),
     "mela_batch_plan_destroy": (None, [_vp]),

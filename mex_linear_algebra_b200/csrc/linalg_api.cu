@@ -3,6 +3,8 @@
 // Host entry points take a MATLAB-layout matrix, run everything on the GPU
 // (pack, eliminate, extract the basis, unpack) and copy the result back.
 // Device entry points are stream-ordered on packed matrices.
+#include <algorithm>
+
 #include "mela_common.cuh"
 #include "mela_internal.h"
 #include "mela_host.h"
@@ -134,6 +136,20 @@ mela_status host_null(const mela_host_matrix *H, int variant, mela_alloc_fn allo
     return null_of_packed((u64 *)P.p, ld, m, n, variant, alloc, ctx, nullity, s);
 }
 
+// Rows of C (rows x w words) with any nonzero word, added to *count.
+__global__ void count_nonzero_rows_kernel(const u64 *__restrict__ C, i64 ldc, i64 rows, i64 w,
+                                          long long *count)
+{
+    long long mine = 0;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < rows; i += (i64)gridDim.x * blockDim.x) {
+        u64 any = 0;
+        for (i64 x = 0; x < w; ++x) any |= C[i * ldc + x];
+        mine += any != 0;
+    }
+    mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd((unsigned long long *)count, (unsigned long long)mine);
+}
+
 }  // namespace mela
 
 using namespace mela;
@@ -241,4 +257,42 @@ extern "C" mela_status mela_dev_unpack_rows(const uint64_t *d_in, int64_t ld, in
         return MELA_ERR_INVALID;
     }
     return launch_unpack_rows((const u64 *)d_in, ld, rows, n, d_out, (cudaStream_t)stream);
+}
+
+extern "C" size_t mela_null_verify_workspace_size(int64_t m, int64_t f)
+{
+    if (m <= 0 || f <= 0) return 0;
+    return (size_t)m * (size_t)words_of(f) * 8;
+}
+
+extern "C" mela_status mela_dev_null_verify(const uint64_t *dA, int64_t lda, int64_t m, int64_t n,
+                                            const uint64_t *dZt, int64_t ldz, int64_t f,
+                                            int64_t *d_bad_rows, void *workspace, size_t workspace_bytes,
+                                            void *stream)
+{
+    if (m < 0 || n < 0 || f < 0 || lda < words_of(n) || ldz < words_of(n)) {
+        set_error("mela_dev_null_verify: bad shape");
+        return MELA_ERR_INVALID;
+    }
+    if (!d_bad_rows || (m > 0 && n > 0 && f > 0 && (!dA || !dZt))) {
+        set_error("mela_dev_null_verify: null pointer");
+        return MELA_ERR_INVALID;
+    }
+    const size_t need = mela_null_verify_workspace_size(m, f);
+    if (workspace_bytes < need || (need && !workspace)) {
+        set_error("mela_dev_null_verify: workspace of %zu bytes needed, %zu given", need, workspace_bytes);
+        return MELA_ERR_INVALID;
+    }
+    const cudaStream_t s = (cudaStream_t)stream;
+    MELA_CUDA_TRY(cudaMemsetAsync(d_bad_rows, 0, sizeof(int64_t), s));
+    if (m == 0 || f == 0) return MELA_OK;
+    // C (m x f) = A (m x n) * Z (n x f); the plain product takes Z^T = Zt as is
+    u64 *C = (u64 *)workspace;
+    const i64 wf = words_of(f);
+    mela_status st = launch_gemm_plain((const u64 *)dA, lda, (const u64 *)dZt, ldz, C, wf, m, n, f, s);
+    if (st != MELA_OK) return st;
+    const i64 blocks = std::min<i64>((m + 255) / 256, (i64)4 * sm_count());
+    count_nonzero_rows_kernel<<<(unsigned)blocks, 256, 0, s>>>(C, wf, m, wf, (long long *)d_bad_rows);
+    MELA_LAUNCH_CHECK("count_nonzero_rows_kernel");
+    return MELA_OK;
 }

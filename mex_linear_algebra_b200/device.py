@@ -82,6 +82,23 @@ def matmul(A: torch.Tensor, B: torch.Tensor, m: int, k: int, n: int, variant: st
     return out
 
 
+def null_verify(A: torch.Tensor, m: int, n: int, Zt: torch.Tensor, f: int, workspace=None,
+                stream=None) -> int:
+    """Number of rows i of A (packed m x n) with A_i . z != 0 for some row z
+    of Zt (packed f x n, a null-space basis as mela_dev_null_basis writes
+    it); 0 means A Z = 0.  Computed on the device."""
+    dev = A.device if A.numel() else Zt.device
+    wsb = int(lib().mela_null_verify_workspace_size(m, f))
+    if workspace is None and wsb:
+        workspace = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    bad = torch.zeros(1, dtype=torch.int64, device=dev)
+    lda = A.shape[1] if A.dim() == 2 else words(n)
+    ldz = Zt.shape[1] if Zt.dim() == 2 else words(n)
+    check(lib().mela_dev_null_verify(_ptr(A), lda, m, n, _ptr(Zt), ldz, f, _ptr(bad), _ptr(workspace),
+                                     workspace.numel() if workspace is not None else 0, _stream(stream)))
+    return int(bad.item())
+
+
 def device_error_flags(clear: bool = True) -> int:
     import ctypes as C
     v = C.c_uint32(0)

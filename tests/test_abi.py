@@ -90,6 +90,24 @@ def test_batch_entry_points_reject_bad_arguments():
     assert L.mela_batch_plan_create(items, 1, -1, None) == _lib.ERR_INVALID
 
 
+def test_null_verify_rejects_bad_arguments():
+    """Shapes, pitches, the result pointer and the workspace are checked
+    before any device work."""
+    from mex_linear_algebra_b200 import _lib
+    L = _lib.lib()
+    assert L.mela_null_verify_workspace_size(100, 70) == 100 * 2 * 8
+    assert L.mela_null_verify_workspace_size(0, 70) == 0
+    assert L.mela_null_verify_workspace_size(100, 0) == 0
+    fake = C.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    assert L.mela_dev_null_verify(fake, 1, -1, 64, fake, 1, 1, fake, None, 0, None) == _lib.ERR_INVALID
+    assert L.mela_dev_null_verify(fake, 1, 4, 130, fake, 3, 1, fake, None, 0, None) == _lib.ERR_INVALID
+    assert L.mela_dev_null_verify(fake, 3, 4, 130, fake, 1, 1, fake, None, 0, None) == _lib.ERR_INVALID
+    assert L.mela_dev_null_verify(fake, 3, 4, 130, fake, 3, 1, None, None, 0, None) == _lib.ERR_INVALID
+    assert L.mela_dev_null_verify(None, 3, 4, 130, fake, 3, 1, fake, fake, 64, None) == _lib.ERR_INVALID
+    assert L.mela_dev_null_verify(fake, 3, 4, 130, fake, 3, 1, fake, fake, 31, None) == _lib.ERR_INVALID
+    assert b"workspace of 32 bytes needed" in L.mela_last_error()
+
+
 def test_workspace_sizes():
     from mex_linear_algebra_b200 import _lib
     L = _lib.lib()

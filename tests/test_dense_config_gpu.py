@@ -74,6 +74,7 @@ def test_dense_rank_and_null_full_size(cuda):
     Z = D.transpose(Zt, f, n)
     prod = D.matmul(A, Z, m, n, f, variant="tc")
     assert int(prod.abs().max().item()) == 0          # A * Z = 0
+    assert D.null_verify(A, m, n, Zt, f) == 0          # the same, by the on-device verifier
     # identity on the free columns: Z restricted to free rows is I
     piv = dpv[:r].cpu().numpy()
     free = np.setdiff1d(np.arange(n), piv)
