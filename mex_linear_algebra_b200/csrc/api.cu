@@ -472,7 +472,7 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
                                                 uint64_t *C, int64_t ldc, i64 m, i64 k, i64 n, int variant,
                                                 cudaStream_t s)
 {
-    cudaStream_t sin, sout;
+    cudaStream_t sin = nullptr, sout = nullptr;
     mela_status st = copy_streams(&sin, &sout);
     if (st != MELA_OK) return st;
     const bool fp4 = variant == MELA_GEMM_TC_FP4;
