@@ -8,6 +8,7 @@
 import os
 
 import numpy as np
+from hypothesis import given, settings, strategies as st
 import pytest
 
 import oracle as O
@@ -135,5 +136,28 @@ def test_oracle_matches_reference_live(shape):
         assert np.array_equal(O.ref_call(fn, X)[0], O.null_logical(X, meth))
     Y = O.unpack(O.rand_dense(98, n, n, m), n, m)
     want = O.unpack(O.matmul(O.pack(X), O.pack(Y), m, n, m), m, m)
+    for fn in ("mela_matmul_gf2", "mela_matmul_m4ri"):
+        assert np.array_equal(O.ref_call(fn, X, Y)[0], want)
+
+
+@ref
+@settings(max_examples=40, deadline=None, derandomize=True)
+@given(m=st.integers(1, 160), n=st.integers(1, 160), density=st.sampled_from([0.01, 0.1, 0.5, 0.9]),
+       dup=st.booleans(), seed=st.integers(0, 2**31 - 1))
+def test_oracle_matches_reference_random(m, n, density, dup, seed):
+    """Sparse, dense and rank-deficient (duplicated rows and columns) inputs:
+    the restatement and the compiled reference agree on all six functions."""
+    rng = np.random.default_rng(seed)
+    X = rng.random((m, n)) < density
+    if dup and m > 1 and n > 1:
+        X[rng.integers(m)] = X[rng.integers(m)]
+        X[:, rng.integers(n)] = X[:, rng.integers(n)]
+    for fn, k in (("mela_rank_gf2", 0), ("mela_rank_m4ri", 10)):
+        assert O.ref_call(fn, X)[0][0, 0] == O.rank(O.pack(X), m, n, k)
+    for fn, meth in (("mela_null_gf2", "gf2"), ("mela_null_m4ri", "m4ri")):
+        assert np.array_equal(O.ref_call(fn, X)[0], O.null_logical(X, meth))
+    p = int(rng.integers(1, 100))
+    Y = rng.random((n, p)) < density
+    want = O.unpack(O.matmul(O.pack(X), O.pack(Y), m, n, p), m, p)
     for fn in ("mela_matmul_gf2", "mela_matmul_m4ri"):
         assert np.array_equal(O.ref_call(fn, X, Y)[0], want)
