@@ -99,17 +99,24 @@ class ClockSampler:
             self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
+        return self.summarize(self.lines)
+
+    @staticmethod
+    def summarize(lines) -> dict:
+        """Median SM clock, the max clock and the throttle reasons seen active
+        in `nvidia-smi --format=csv,noheader,nounits` lines of FIELDS."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                smax = float(parts[1])
+                cur, mx = float(parts[0]), float(parts[1])
             except ValueError:
                 continue
+            sm.append(cur)
+            smax = mx
             for nm, v in zip(names, parts[4:8]):
                 if v.lower() == "active":
                     reasons.add(nm)
