@@ -93,6 +93,17 @@ const char *mela_status_string(mela_status s);
 const char *mela_last_error(void);
 /* Device-side error bits (timeouts of bounded waits); `clear` resets them. */
 mela_status mela_device_error_flags(uint32_t *flags, int clear);
+/* Diagnostic of the failure path (no reference counterpart): one kernel whose
+ * wait nothing will satisfy -- kind 0 a device flag, kind 1 an mbarrier with
+ * tensor memory held -- runs out after limit_ns (1 us .. 1 s), sets the
+ * timeout bit of the device error word, frees what it holds and returns.
+ * d_out (device, 2 words): [0] = 1 when the wait ran out, [1] = 1 when kind
+ * 1 freed its tensor memory.  sync = 0: stream-ordered, the bit stays set
+ * for mela_device_error_flags; sync = 1: waits for the stream and returns
+ * MELA_ERR_TIMEOUT, clearing the bit, as every synchronous entry point does
+ * after a timed-out wait. */
+mela_status mela_diag_wait_timeout(int32_t kind, uint64_t limit_ns, uint32_t *d_out, int32_t sync,
+                                   void *stream);
 
 /* ------------------------------------------------------------------ */
 /* host entry points (MATLAB layout in, MATLAB layout out)              */

@@ -65,6 +65,7 @@ SIGNATURES = {
     "mela_status_string": (C.c_char_p, [_st]),
     "mela_last_error": (C.c_char_p, []),
     "mela_device_error_flags": (_st, [C.POINTER(_u32), C.c_int]),
+    "mela_diag_wait_timeout": (_st, [_i32, _u64, _vp, _i32, _vp]),
     "mela_matmul_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
     "mela_matmul_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
     "mela_rank_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(C.c_double)]),

@@ -59,6 +59,17 @@ __device__ __forceinline__ unsigned long long global_ns()
 // ---------------------------------------------------------------- launch sizing
 int sm_count();  // multiprocessors of the current device (cached per device)
 
+// A grid's y and z extents are limited to 65535 blocks: larger shapes are
+// refused up front (MELA_ERR_UNSUPPORTED) instead of failing at launch.
+inline mela_status check_grid_yz(i64 y, i64 z, const char *what)
+{
+    if (y > 65535 || z > 65535) {
+        set_error("%s: shape needs a grid of %lld x %lld blocks in y and z (limit 65535)", what, y, z);
+        return MELA_ERR_UNSUPPORTED;
+    }
+    return MELA_OK;
+}
+
 // 32 x 32 bit transpose across a warp: lane r passes row r (bit c = column
 // c); lane c gets column c (bit r = row r).  Five rounds of shuffle
 // butterflies: at round s the lanes with bit s clear trade their columns

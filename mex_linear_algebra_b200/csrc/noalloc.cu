@@ -17,7 +17,10 @@
 // Host code cannot use the array's name as a device address (on the host it
 // names a host-side shadow), so the first call on each device looks the
 // address up with cudaGetSymbolAddress, with that device current, and caches
-// it.  That first call should therefore come before any stream capture.
+// it.  That first call should therefore come before any stream capture.  The
+// cache is keyed on the device's current CUDA context: after a device reset
+// (a new primary context, where the module may load at another address) the
+// next call looks the address up again.
 //
 // All calls share the one array and it keeps whatever the last call left in
 // it.  Nothing in it needs to start at zero: the transpose kernel writes
@@ -25,6 +28,8 @@
 // the GPU (different streams, or different host threads, on the same device)
 // race on the array; serialise them.
 #include <mutex>
+
+#include <cuda.h>
 
 #include "mela_common.cuh"
 #include "mela_internal.h"
@@ -40,9 +45,38 @@ namespace {
 constexpr int kMaxDev = 64;
 std::mutex g_mu;
 void *g_scratch_addr[kMaxDev];
+unsigned long long g_scratch_ctx[kMaxDev];  // id of the context the address belongs to
+
+// Unique id of the calling thread's current context (0 when there is none).
+// The driver functions are looked up through the runtime, so the library
+// loads on machines without the driver.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) != cudaSuccess ||
+            r1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) != cudaSuccess ||
+            r2 != cudaDriverEntryPointSuccess)
+            return 0;
+        get_current = (CtxGetCurrentFn)p;
+        get_id = (CtxGetIdFn)q;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 }  // namespace
 
-// Device address of g_static_scratch on the current device (looked up once).
+// Device address of g_static_scratch on the current device, looked up once
+// per device and context.
 static mela_status static_scratch(void **out)
 {
     int d = 0;
@@ -52,11 +86,14 @@ static mela_status static_scratch(void **out)
         return MELA_ERR_UNSUPPORTED;
     }
     std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_addr[d]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[d] || ctx == 0 || ctx != g_scratch_ctx[d]) {
+        // the lookup also makes the device's primary context current
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess || !p) return cuda_status(e, "cudaGetSymbolAddress(g_static_scratch)");
         g_scratch_addr[d] = p;
+        g_scratch_ctx[d] = current_context_id();
     }
     *out = g_scratch_addr[d];
     return MELA_OK;
@@ -90,6 +127,11 @@ extern "C" mela_status mela_dev_matmul_plain_static(const uint64_t *dA, int64_t 
                   need, kMaxScratchBytes);
         return MELA_ERR_UNSUPPORTED;
     }
+    // launch shapes of the transpose (k / 256 row blocks) and of the product
+    // (m / 128 row tiles) are checked before any device work
+    if (mela_status st = check_grid_yz((k + 255) / 256, (m + 127) / 128, "mela_dev_matmul_plain_static");
+        st != MELA_OK)
+        return st;
     cudaStream_t s = (cudaStream_t)stream;
     if (k == 0) {
         MELA_CUDA_TRY(cudaMemset2DAsync(dC, (size_t)ldc * 8, 0, (size_t)words_of(n) * 8, (size_t)m, s));

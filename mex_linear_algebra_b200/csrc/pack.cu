@@ -313,6 +313,7 @@ mela_status launch_expand_t(const u64 *in, i64 ld, i64 kbits, i64 cols, i64 cols
         return MELA_ERR_INVALID;
     }
     const i64 kvals = fp4 ? 2 * kpad : kpad;
+    if (mela_status st = check_grid_yz((kvals + 255) / 256, 1, "expand_t"); st != MELA_OK) return st;
     dim3 grid((unsigned)(cols_pad / 256), (unsigned)((kvals + 255) / 256));
     if (fp4)
         expand_t_kernel<true><<<grid, 256, 0, s>>>(in, ld, kbits, cols, kpad, out);
@@ -326,6 +327,7 @@ mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *
                              cudaStream_t s)
 {
     if (rows <= 0 || cols <= 0) return MELA_OK;
+    if (mela_status st = check_grid_yz((rows + 255) / 256, 1, "transpose"); st != MELA_OK) return st;
     dim3 grid((unsigned)words_of(cols), (unsigned)((rows + 255) / 256));
     transpose_kernel<<<grid, 256, 0, s>>>(in, ld_in, rows, cols, out, ld_out);
     MELA_LAUNCH_CHECK("transpose_kernel");
@@ -337,6 +339,7 @@ mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld
     if (m <= 0) return MELA_OK;
     i64 wgroups = (ld + 7) / 8;
     if (wgroups == 0) return MELA_OK;
+    if (mela_status st = check_grid_yz(wgroups, 1, "pack"); st != MELA_OK) return st;
     dim3 grid((unsigned)((m + 31) / 32), (unsigned)wgroups);
     if (kind == MELA_KIND_DOUBLE)
         pack_kernel<double><<<grid, 256, 0, s>>>((const double *)in, m, n, out, ld);
@@ -349,6 +352,7 @@ mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld
 mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *out, cudaStream_t s)
 {
     if (m <= 0 || n <= 0) return MELA_OK;
+    if (mela_status st = check_grid_yz((words_of(n) + 7) / 8, 1, "unpack"); st != MELA_OK) return st;
     dim3 grid((unsigned)((m + 31) / 32), (unsigned)((words_of(n) + 7) / 8));
     unpack_kernel<<<grid, 256, 0, s>>>(in, ld, m, n, out);
     MELA_LAUNCH_CHECK("unpack_kernel");

@@ -56,15 +56,16 @@ __device__ __forceinline__ bool mbar_try_wait(u64 *bar, u32 parity)
 }
 
 // Bounded wait for phase `parity` of `bar`.  Returns false (and sets the
-// timeout bit in *err) if the phase did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(u64 *bar, u32 parity, u32 *err)
+// timeout bit in *err) if the phase did not complete within `limit_ns`.
+__device__ __forceinline__ bool mbar_wait(u64 *bar, u32 parity, u32 *err,
+                                          unsigned long long limit_ns = kWaitLimitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {
         for (int i = 0; i < 64; ++i)
             if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > kWaitLimitNs) {
+        if (global_ns() - t0 > limit_ns) {
             if (err) atomicOr(err, kErrWaitTimeout);
             return false;
         }

@@ -161,3 +161,42 @@ def test_tc_rref_matches_blocked(cuda, shape, rank):
         assert np.array_equal(pa, pb)
         if rref:
             assert np.array_equal(_rref_rows(Ma, m, n, ra, qa), _rref_rows(Mb, m, n, rb, qb))
+
+
+def test_tc_graph_replay_follows_the_data(cuda):
+    """The tensor-core form replays its launch sequence as a CUDA graph from
+    the second call with the same buffers on.  The sequence must not depend
+    on the data: the same matrix buffer, workspace and outputs get inputs of
+    full rank, lower rank and rank 0 in turn (rank and RREF), and every call
+    matches the oracle."""
+    import torch
+    from mex_linear_algebra_b200 import _lib, device as D
+    L = _lib.lib()
+    m, n = 700, 1400  # six 256-column windows
+    Lr = D.rand_dense(47, 0, m, 250)
+    Rr = D.rand_dense(47, 1, 250, n)
+    inputs = [O.rand_dense(47, 2, m, n),
+              to_host(D.matmul(Lr, Rr, m, 250, n, variant="plain")),
+              np.zeros((m, (n + 63) // 64), dtype=np.uint64),
+              O.rand_dense(47, 3, m, n),
+              to_host(D.matmul(Lr, Rr, m, 250, n, variant="plain"))]
+    M = torch.empty((m, (n + 63) // 64), dtype=torch.int64, device="cuda")
+    rank = torch.zeros(1, dtype=torch.int64, device="cuda")
+    piv = torch.empty(m, dtype=torch.int64, device="cuda")
+    prow = torch.empty(m, dtype=torch.int64, device="cuda")
+    wsb = L.mela_elim_workspace_size(m, n)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    for rref in (False, True):
+        fn = L.mela_dev_rref if rref else L.mela_dev_rank
+        for P in inputs:
+            want_R, want_piv = O.rref(P, m, n)
+            M.copy_(to_dev(P))
+            _lib.check(fn(_lib.ELIM_TC, M.data_ptr(), M.shape[1], m, n, rank.data_ptr(), piv.data_ptr(),
+                          prow.data_ptr(), ws.data_ptr(), wsb, s))
+            r = int(rank.item())
+            assert r == len(want_piv)
+            assert np.array_equal(to_host(piv)[:r].astype(np.int64), want_piv)
+            if rref:
+                rows = to_host(M)[to_host(prow)[:r].astype(np.int64)]
+                assert np.array_equal(valid_words(rows, n), valid_words(want_R[:r], n))

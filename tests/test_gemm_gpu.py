@@ -121,14 +121,32 @@ def test_variants_agree_4096(cuda):
 
 
 def test_large_config_checks(cuda):
-    """32768^3 (seed 1): tensor-core and plain forms agree bit for bit, and
+    """32768^3 (seed 1): the FP4 and INT8 tensor-core forms and the plain form
+    all reproduce the checker's digest of the full product (computed on the
+    CPU by the oracle and by the reference's own mela_matmul_gf2,
+    tests/golden/make_config_digests.py), row block by row block, and
     (A*B)*X == A*(B*X) for a random 32768 x 64 block X."""
+    import hashlib
+    import json
+    import os
     import torch
     D = _dev()
+    g = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "config_digests.json")))["product_32768"]
     m = k = n = 32768
     A = D.rand_dense(1, 0, m, k)
     B = D.rand_dense(1, 1, k, n)
+
+    def blocks(C):
+        h = C.cpu().numpy()
+        rb = g["row_block"]
+        return [hashlib.blake2b(h[i:i + rb].tobytes(), digest_size=16).hexdigest() for i in range(0, m, rb)]
+
+    c_fp4 = D.matmul(A, B, m, k, n, variant="tc_fp4")
+    assert blocks(c_fp4) == g["block_digests"]
     c_tc = D.matmul(A, B, m, k, n, variant="tc")
+    assert torch.equal(c_tc, c_fp4)
+    del c_fp4
     c_plain = D.matmul(A, B, m, k, n, variant="plain")
     assert torch.equal(c_tc, c_plain)
     X = D.rand_dense(1, 2, n, 64)

@@ -161,3 +161,28 @@ def test_oracle_matches_reference_random(m, n, density, dup, seed):
     want = O.unpack(O.matmul(O.pack(X), O.pack(Y), m, n, p), m, p)
     for fn in ("mela_matmul_gf2", "mela_matmul_m4ri"):
         assert np.array_equal(O.ref_call(fn, X, Y)[0], want)
+
+
+@settings(max_examples=30, deadline=None, derandomize=True)
+@given(m=st.integers(1, 200), n=st.integers(1, 300), density=st.sampled_from([0.05, 0.5]),
+       seed=st.integers(0, 2**31 - 1))
+def test_null_basis_read_off_the_rref(m, n, density, seed):
+    """The identity the full-size null-space digest relies on
+    (tests/golden/make_config_digests.py): the back-substituted basis equals
+    the one read off the RREF -- vector i has bit f_i and, at pivot column
+    c_p, the RREF's bit (p, f_i)."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "make_config_digests", os.path.join(os.path.dirname(__file__), "golden", "make_config_digests.py"))
+    MD = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(MD)
+    rng = np.random.default_rng(seed)
+    X = rng.random((m, n)) < density
+    if m > 2:
+        X[rng.integers(m)] = X[rng.integers(m)]
+    P = O.pack(X)
+    R, piv = O.rref(P, m, n)
+    want = O.null_basis_packed(P, m, n)
+    got = MD.null_from_rref(R, piv, n)
+    assert np.array_equal(got, want)
