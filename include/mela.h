@@ -78,11 +78,28 @@ typedef enum {
 typedef enum {
     MELA_ELIM_AUTO = 0,
     MELA_ELIM_PLAIN = 1,  /* per-pivot warp-ballot search + broadcast-XOR sweep */
-    MELA_ELIM_M4RI = 2,   /* 64-column panels, 8-bit Gray-code tables in shared memory */
+    MELA_ELIM_M4RI = 2,   /* 64-column panels, Four-Russians tables in shared memory (k = 8 unless tuned) */
     MELA_ELIM_M4RI_K4 = 3, /* the same panels with 4-bit tables (M4RI k = 4) */
     MELA_ELIM_FUSED = 4,   /* the whole elimination by one CTA in one launch */
     MELA_ELIM_TC = 5       /* 256-column windows, trailing update on the tensor cores (tcgen05 kind::i8) */
 } mela_elim_variant;
+
+/* Tuning fields of a variant argument.  A variant argument is a base
+ * variant (above) in bits 0-7, optionally ORed with these fields; a field of
+ * 0 keeps the variant's default.  They change how a result is computed,
+ * never the result.  The reference fixes its Four-Russians k per function
+ * (k = 8 in src/mela_matmul_m4ri.c:33 and src/mela_null_m4ri.c:28, k = 10
+ * in src/mela_rank_m4ri.c:18); here it is a parameter.
+ *   MELA_TUNE_K(k)     MELA_ELIM_M4RI: table width k in {4, 6, 7, 8, 9, 10}
+ *                      (MELA_ELIM_M4RI_K4 takes only 4; MELA_GEMM_M4RI only 8).
+ *   MELA_TUNE_TILE(t)  MELA_ELIM_M4RI / _K4: rows per update CTA, t = 1: 256,
+ *                      2: 1024 (default), 3: 4096.
+ *                      MELA_GEMM_TC / _TC_FP4: t = 1: one CTA per 128 x 256
+ *                      tile; 2: CTA pairs per 256 x 256 tile (the default
+ *                      where the padded row count allows). */
+#define MELA_VARIANT_BASE(v) ((int32_t)(v) & 0xff)
+#define MELA_TUNE_K(k) ((int32_t)(k) << 8)
+#define MELA_TUNE_TILE(t) ((int32_t)(t) << 12)
 
 /* ------------------------------------------------------------------ */
 /* library                                                             */
@@ -314,6 +331,19 @@ typedef struct mela_batch_plan mela_batch_plan;
  * with the CTA / 128-thread / warp engine (for testing the engines). */
 mela_status mela_batch_plan_create(const mela_batch_item *items, int64_t count,
                                    int32_t force_class, mela_batch_plan **plan);
+/* The same with the engine policy -2 available: each matrix goes to the
+ * engine the installed cost model prices lowest among those whose shared
+ * memory it fits, from its shape, its density (densities[i], the fraction of
+ * ones; NULL: 0.5 for all) and the batch mix (the matrix count and mean
+ * log2(m*n) of this batch) -- the size rule of policy -1 when no model is
+ * installed.  Policies -1, 0, 1, 2 as force_class above. */
+mela_status mela_batch_plan_create_ex(const mela_batch_item *items, int64_t count,
+                                      const double *densities, int32_t policy,
+                                      mela_batch_plan **plan);
+/* d_counts[i] = number of ones of item i of a packed batch (in_offset
+ * layout), stream-ordered: the densities mela_batch_plan_create_ex takes. */
+mela_status mela_batch_popcounts(const mela_batch_item *items, int64_t count, const uint64_t *d_in,
+                                 int64_t *d_counts, void *stream);
 void mela_batch_plan_destroy(mela_batch_plan *plan);
 mela_status mela_batch_plan_stats(const mela_batch_plan *plan, int64_t *big, int64_t *mid,
                                   int64_t *small);
@@ -338,24 +368,35 @@ mela_status mela_batch_unpack_logical(mela_batch_plan *plan, const uint64_t *d_p
 /* learned dispatch: the cost model                                      */
 /* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  A small MLP predicts the log2 running
- * time (microseconds) of each of a request's kernel variants from its
- * shape and density; the dispatcher takes the fastest prediction.  It only
- * chooses how a result is computed: every variant returns the same bits.
- * Parameters: one float array W1[8][32] b1[32] W2[32][32] b2[32] W3[32][5]
- * b3[5].  Variant order per output: products (plain, m4ri, tc, tc_fp4; the
- * fifth output unused); rank and null space (plain, m4ri, m4ri_k4, fused, tc). */
-#define MELA_MLP_IN 8
+ * time (microseconds) of each configuration of a request -- a variant with
+ * its tuning fields, or for a matrix inside a batched launch the engine
+ * that runs it -- from the request's shape, density and batch mix; the
+ * dispatcher takes the fastest prediction.  It only chooses how a result is
+ * computed: every configuration returns the same bits.
+ * Inputs (MELA_MLP_IN): log2 m, log2 n, log2 p (products), density, the op
+ * (rank, null space, product, batched rank + null space: one-hot), log2 of
+ * the number of matrices in the batch, and the batch mix: the mean
+ * log2(m * n) over the batch.  Outputs: one per configuration of the op
+ * (mela_costmodel_config).  Parameters: one float array
+ * W1[IN][H1] b1[H1] W2[H1][H2] b2[H2] W3[H2][OUT] b3[OUT]. */
+#define MELA_MLP_IN 10
 #define MELA_MLP_H1 32
 #define MELA_MLP_H2 32
-#define MELA_MLP_OUT 5
-#define MELA_MLP_PARAMS 1509
-typedef enum { MELA_OP_RANK = 0, MELA_OP_NULL = 1, MELA_OP_MATMUL = 2 } mela_op;
+#define MELA_MLP_OUT 10
+#define MELA_MLP_PARAMS 1738
+typedef enum { MELA_OP_RANK = 0, MELA_OP_NULL = 1, MELA_OP_MATMUL = 2, MELA_OP_BATCH = 3 } mela_op;
 
-/* Y (N x 5) = network(X (N x 8)) on the device. */
+/* Configurations of an op, in the model's output order: their count, and
+ * the variant argument of configuration `index` (for MELA_OP_BATCH the
+ * batch engine: 0 = a CTA, 1 = a 128-thread group, 2 = a warp per matrix);
+ * -1 when out of range. */
+int32_t mela_costmodel_config_count(int32_t op);
+int32_t mela_costmodel_config(int32_t op, int32_t index);
+/* Y (N x OUT) = network(X (N x IN)) on the device. */
 mela_status mela_mlp_forward(const float *d_params, const float *d_X, int64_t N, float *d_Y,
                              void *stream);
 /* d_grad = gradient of the masked mean squared error between the network's
- * outputs and targets T (N x 5, mask 1 where observed), scaled by inv_count
+ * outputs and targets T (N x OUT, mask 1 where observed), scaled by inv_count
  * = 1/(observed count); d_loss_sum (optional) = sum of squared errors. */
 mela_status mela_mlp_gradient(const float *d_params, const float *d_X, const float *d_T,
                               const float *d_mask, int64_t N, float inv_count, float *d_grad,
@@ -365,12 +406,22 @@ mela_status mela_mlp_adam_step(float *d_params, const float *d_grad, float *d_m1
                                int64_t step, float lr, void *stream);
 /* Install (or, with NULL, remove) the dispatch model from host memory. */
 mela_status mela_costmodel_load(const float *h_params);
-/* Variant index (0..3 for products, 0..4 otherwise) the installed model picks, or -1 when none is
- * installed (the fixed rule is used then). */
-int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density);
-/* The 8 input features of a request. */
+/* Configuration index the installed model picks for a request, or -1 when
+ * none is installed (the dispatcher then uses its fixed rule).  Single calls
+ * pass batch_count = 1 and batch_log2_cells = log2(m * n). */
+int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density,
+                              int64_t batch_count, double batch_log2_cells);
+/* The MELA_MLP_IN input features of a request. */
 void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
-                             float *x);
+                             int64_t batch_count, double batch_log2_cells, float *x);
+/* Number of ones of the packed m x n device matrix into *d_count (device),
+ * stream-ordered: the density the dispatcher feeds the model.  The AUTO
+ * variants of mela_dev_matmul / mela_dev_rank / mela_dev_rref measure it
+ * this way when a model is installed -- which waits for the stream (the
+ * count is read back) unless the stream is being captured, where 0.5 is
+ * assumed. */
+mela_status mela_dev_popcount(const uint64_t *dM, int64_t ld, int64_t m, int64_t n, int64_t *d_count,
+                              void *stream);
 
 /* ------------------------------------------------------------------ */
 /* allocation-free product                                              */

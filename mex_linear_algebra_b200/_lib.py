@@ -25,10 +25,13 @@ GEMM_VARIANTS = {"auto": GEMM_AUTO, "plain": GEMM_PLAIN, "m4ri": GEMM_M4RI, "tc"
 # mela_function (gateway ids)
 FN_MATMUL_GF2, FN_MATMUL_M4RI, FN_RANK_GF2, FN_RANK_M4RI, FN_NULL_GF2, FN_NULL_M4RI = range(6)
 # mela_op and the cost model's shape
-OP_RANK, OP_NULL, OP_MATMUL = 0, 1, 2
-MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 8, 32, 32, 5, 1509
-# variant index (model output) -> variant code, per op
-OP_VARIANTS = {OP_MATMUL: (1, 2, 3, 4), OP_RANK: (1, 2, 3, 4), OP_NULL: (1, 2, 3, 4)}
+OP_RANK, OP_NULL, OP_MATMUL, OP_BATCH = 0, 1, 2, 3
+MLP_IN, MLP_H1, MLP_H2, MLP_OUT, MLP_PARAMS = 10, 32, 32, 10, 1738
+
+
+# tuning fields of a variant argument (MELA_TUNE_K / MELA_TUNE_TILE)
+def tune(base: int, k: int = 0, tile: int = 0) -> int:
+    return base | (k << 8) | (tile << 12)
 # mela_elim_variant
 ELIM_AUTO, ELIM_PLAIN, ELIM_M4RI, ELIM_M4RI_K4, ELIM_FUSED, ELIM_TC = 0, 1, 2, 3, 4, 5
 ELIM_VARIANTS = {"auto": ELIM_AUTO, "plain": ELIM_PLAIN, "m4ri": ELIM_M4RI, "m4ri_k4": ELIM_M4RI_K4,
@@ -106,8 +109,13 @@ SIGNATURES = {
     "mela_mlp_gradient": (_st, [_vp, _vp, _vp, _vp, _i64, C.c_float, _vp, _vp, _vp]),
     "mela_mlp_adam_step": (_st, [_vp, _vp, _vp, _vp, _i64, C.c_float, _vp]),
     "mela_costmodel_load": (_st, [_vp]),
-    "mela_costmodel_choose": (_i32, [_i32, _i64, _i64, _i64, C.c_double]),
-    "mela_costmodel_features": (None, [_i32, _i64, _i64, _i64, C.c_double, _vp]),
+    "mela_costmodel_choose": (_i32, [_i32, _i64, _i64, _i64, C.c_double, _i64, C.c_double]),
+    "mela_costmodel_features": (None, [_i32, _i64, _i64, _i64, C.c_double, _i64, C.c_double, _vp]),
+    "mela_costmodel_config_count": (_i32, [_i32]),
+    "mela_costmodel_config": (_i32, [_i32, _i32]),
+    "mela_dev_popcount": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),
+    "mela_batch_plan_create_ex": (_st, [C.POINTER(BatchItem), _i64, _vp, _i32, C.POINTER(_vp)]),
+    "mela_batch_popcounts": (_st, [C.POINTER(BatchItem), _i64, _vp, _vp, _vp]),
     "mela_static_scratch_bytes": (_sz, []),
     "mela_dev_matmul_plain_static": (_st, [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp]),
 }

@@ -1,12 +1,20 @@
-"""Exhaustive autotuner: time every kernel variant of a request on the GPU.
+"""Exhaustive autotuner: time every configuration of a request on the GPU.
 
-For each request (op, m, n, p, density) the inputs are generated on the
-device from the seeded Bernoulli generator, every variant runs once to warm
-up and ``reps`` times under CUDA events, and the median is recorded in
-microseconds.  The variants' results are compared with each other (they must
-be bit-identical) and the record says so.  Records form the timing database
-the cost model is trained on, and the exhaustive best time of each request is
-the judge of the model's regret.
+A configuration is a kernel variant with its tuning fields (Four-Russians k
+and update row tile for the blocked elimination, single CTAs or CTA pairs
+for the tensor-core products), or, for a matrix inside a batched launch, the
+engine that runs it.  For each request the inputs are generated on the
+device from the seeded Bernoulli generator, every configuration runs once to
+warm up and ``reps`` times under CUDA events, and the median is recorded in
+microseconds.  The results are compared with each other (they must be
+bit-identical) and the record says so.  Records form the timing database
+the cost model is trained on, and the exhaustive best time of each request
+is the judge of the model's regret.
+
+Requests: the mixed stream of rank, null-space and product requests (m, n,
+p log-uniform in [32, 8192], density log-uniform in [0.001, 0.5],
+``gen.mixed_stream``) and batch requests (``gen.batch_requests``: a batch of
+`count` m x n Bernoulli matrices; per-matrix time of each engine).
 
     python -m mex_linear_algebra_b200.autotune --count 600 --offset 100000 --out db.json
 """
@@ -20,9 +28,10 @@ import numpy as np
 
 from . import _lib, gen
 from ._lib import check, lib
-from .costmodel import VARIANT_NAMES
+from .costmodel import CONFIG_NAMES, config_codes
 
 SEED = 4
+SLOW_US = 200_000.0  # a configuration slower than this is timed once, not `reps` times
 
 
 def _events(torch):
@@ -37,15 +46,38 @@ def _bernoulli(torch, seed, stream_id, m, n, density):
     return t
 
 
-def time_matmul(torch, m, k, n, density, stream_id, reps=3):
+def _time(torch, fn, reps, setup=None):
+    """Median of `reps` CUDA-event timings (us) after one untimed call; a
+    call slower than SLOW_US is timed once."""
+    if setup:
+        setup()
+    fn()
+    ts = []
+    for _ in range(reps):
+        if setup:
+            setup()
+        e0, e1 = _events(torch)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1) * 1e3)
+        if ts[-1] > SLOW_US:
+            break
+    return float(np.median(ts))
+
+
+def time_matmul(torch, m, k, n, density, stream_id, reps=3, extra=None):
+    """Every product configuration (and the `extra` variant arguments, e.g.
+    AUTO) on one request: (times by name, all results identical)."""
     L = lib()
     s = torch.cuda.current_stream().cuda_stream
     A = _bernoulli(torch, SEED, 2 * stream_id, m, k, density)
     B = _bernoulli(torch, SEED, 2 * stream_id + 1, k, n, density)
     wn = (n + 63) // 64
     times, outs = {}, {}
-    for v, name in zip((_lib.GEMM_PLAIN, _lib.GEMM_M4RI, _lib.GEMM_TC, _lib.GEMM_TC_FP4),
-                       VARIANT_NAMES["matmul"]):
+    todo = list(zip(CONFIG_NAMES["matmul"], config_codes("matmul"))) + list((extra or {}).items())
+    for name, v in todo:
         wsb = L.mela_matmul_workspace_size(v, m, k, n)
         ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
         C_ = torch.empty((m, wn), dtype=torch.int64, device="cuda")
@@ -53,22 +85,16 @@ def time_matmul(torch, m, k, n, density, stream_id, reps=3):
         def run():
             check(L.mela_dev_matmul(v, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
                                     C_.data_ptr(), wn, m, k, n, ws.data_ptr(), wsb, s))
-        run()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = _events(torch)
-            e0.record()
-            run()
-            e1.record()
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1) * 1e3)
-        times[name] = float(np.median(ts))
+        times[name] = _time(torch, run, reps)
         outs[name] = C_
+        del ws
     agree = all(torch.equal(outs[x], outs["plain"]) for x in outs)
     return times, agree
 
 
-def time_elim(torch, op, m, n, density, stream_id, reps=3):
+def time_elim(torch, op, m, n, density, stream_id, reps=3, extra=None):
+    """Every elimination configuration (rank, or RREF + null-space basis for
+    op 'null'), plus the `extra` variant arguments."""
     L = lib()
     s = torch.cuda.current_stream().cuda_stream
     A0 = _bernoulli(torch, SEED, 2 * stream_id, m, n, density)
@@ -79,66 +105,88 @@ def time_elim(torch, op, m, n, density, stream_id, reps=3):
     rank = torch.zeros(1, dtype=torch.int64, device="cuda")
     piv = torch.empty(mn, dtype=torch.int64, device="cuda")
     prow = torch.empty(mn, dtype=torch.int64, device="cuda")
+    M = A0.clone()
+    Zt = torch.empty((max(n, 1), wc), dtype=torch.int64, device="cuda")
+    nwb = L.mela_null_workspace_size(n, min(m, n))  # the largest null-space workspace (full rank)
+    nws = torch.empty(max(nwb, 1), dtype=torch.uint8, device="cuda")
+    fn = L.mela_dev_rref if op == "null" else L.mela_dev_rank
     times, results = {}, {}
-    for v, name in zip((_lib.ELIM_PLAIN, _lib.ELIM_M4RI, _lib.ELIM_M4RI_K4, _lib.ELIM_FUSED, _lib.ELIM_TC),
-                       VARIANT_NAMES[op]):
-        ts = []
-        for rep in range(reps + 1):
-            M = A0.clone()
-            torch.cuda.synchronize()
-            e0, e1 = _events(torch)
-            e0.record()
-            fn = L.mela_dev_rref if op == "null" else L.mela_dev_rank
+    todo = list(zip(CONFIG_NAMES[op], config_codes(op))) + list((extra or {}).items())
+    for name, v in todo:
+        def setup():
+            M.copy_(A0)
+
+        def run():
             check(fn(v, M.data_ptr(), wc, m, n, rank.data_ptr(), piv.data_ptr(), prow.data_ptr(),
                      ws.data_ptr(), wsb, s))
-            e1.record()
-            e1.synchronize()
-            t = e0.elapsed_time(e1) * 1e3
-            r = int(rank.item())
-            res = (r,)
             if op == "null":
-                f = n - r
-                Zt = torch.empty((max(f, 1), wc), dtype=torch.int64, device="cuda")
-                nwb = L.mela_null_workspace_size(n, r)
-                nws = torch.empty(max(nwb, 1), dtype=torch.uint8, device="cuda")
-                e2, e3 = _events(torch)
-                e2.record()
+                r = int(rank.item())
                 check(L.mela_dev_null_basis(M.data_ptr(), wc, m, n, r, piv.data_ptr(), prow.data_ptr(),
                                             Zt.data_ptr(), wc, nws.data_ptr(), nwb, s))
-                e3.record()
-                e3.synchronize()
-                t += e2.elapsed_time(e3) * 1e3
-                res = (r, Zt[:f].clone())
-            if rep > 0:
-                ts.append(t)
-        times[name] = float(np.median(ts))
-        results[name] = res
+        times[name] = _time(torch, run, reps, setup)
+        r = int(rank.item())
+        results[name] = (r, Zt[:n - r].clone() if op == "null" else None)
     base = results["plain"]
-    agree = True
-    for x in results.values():
-        if x[0] != base[0]:
-            agree = False
-        elif op == "null" and not torch.equal(x[1], base[1]):
-            agree = False
+    agree = all(x[0] == base[0] and (op != "null" or torch.equal(x[1], base[1])) for x in results.values())
     return times, agree
 
 
-def time_request(req, reps=3):
+def time_batch(torch, m, n, density, count, stream_id, reps=3):
+    """A batch of `count` m x n Bernoulli(density) matrices (one device
+    stream, stacked: the packed batch layout) run with each engine forced;
+    per-matrix microseconds by engine name, the engine the size rule picks,
+    and whether every engine gave the same ranks and bases."""
+    from .device import BatchPlan
+    s_ = [(m, n)] * count
+    d_in = _bernoulli(torch, SEED, 100000 + stream_id, count * m, n, density).reshape(-1)
+    times, outs, rule = {}, {}, None
+    base = BatchPlan(s_)
+    st = base.stats()
+    rule = "cta" if st["cta"] == count else "group" if st["group128"] == count else "warp"
+    base.close()
+    for c, name in enumerate(CONFIG_NAMES["batch"]):
+        plan = BatchPlan(s_, force_class=c)
+        st = plan.stats()
+        if st[("cta", "group128", "warp")[c]] != count:  # the matrices do not fit that engine
+            plan.close()
+            continue
+        ranks, zt = plan.outputs()
+        zt.zero_()  # words past each basis stay zero, so whole buffers compare
+
+        def run():
+            plan.run(d_in, ranks, zt)
+        times[name] = _time(torch, run, reps) / count
+        outs[name] = (ranks.clone(), zt.clone())
+        plan.close()
+        del ranks, zt
+    first = next(iter(outs.values()))
+    agree = all(torch.equal(o[0], first[0]) and torch.equal(o[1], first[1]) for o in outs.values())
+    return times, rule, agree
+
+
+def time_request(req, reps=3, extra=None):
     import torch
     op, m, n, p, d, sid = req["op"], req["m"], req["n"], req.get("p", 0), req["density"], req["stream"]
-    if op == "matmul":
-        times, agree = time_matmul(torch, m, n, p, d, sid, reps)
-    else:
-        times, agree = time_elim(torch, op, m, n, d, sid, reps)
     out = dict(req)
+    if op == "matmul":
+        times, agree = time_matmul(torch, m, n, p, d, sid, reps, extra)
+    elif op == "batch":
+        times, rule, agree = time_batch(torch, m, n, d, req["batch_count"], sid, reps)
+        out["rule"] = rule
+        out["batch_log2_cells"] = float(np.log2(max(m * n, 1)))
+    else:
+        times, agree = time_elim(torch, op, m, n, d, sid, reps, extra)
     out["times_us"] = times
     out["agree"] = bool(agree)
     return out
 
 
-def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 4e7, verbose: bool = False):
-    """Time `count` requests of the mixed stream starting at request `offset`.
-    Requests whose matrices exceed `max_cells` bits are skipped (bounded run)."""
+def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 7e7, batch_count: int = 0,
+             verbose: bool = False):
+    """Time `count` requests of the mixed stream from request `offset` on
+    (requests above `max_cells` bits are skipped; the stream's largest,
+    8192 x 8192, is 6.7e7), then `batch_count` batch requests."""
+    import torch
     reqs = gen.mixed_stream(offset + count, SEED)[offset:]
     db = []
     t0 = time.time()
@@ -149,6 +197,12 @@ def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 4e7, ver
         db.append(time_request(r, reps))
         if verbose and (i + 1) % 50 == 0:
             print(f"{i + 1}/{count} timed, {time.time() - t0:.1f}s", flush=True)
+        torch.cuda.empty_cache()
+    for j, r in enumerate(gen.batch_requests(batch_count, SEED, offset)):
+        db.append(time_request(r, reps))
+        torch.cuda.empty_cache()
+        if verbose and (j + 1) % 25 == 0:
+            print(f"batch {j + 1}/{batch_count} timed, {time.time() - t0:.1f}s", flush=True)
     return db
 
 
@@ -156,13 +210,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--count", type=int, default=600)
     ap.add_argument("--offset", type=int, default=100000)
+    ap.add_argument("--batches", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--out", default="autotune_db.json")
     a = ap.parse_args()
-    db = build_db(a.count, a.offset, a.reps, verbose=True)
+    db = build_db(a.count, a.offset, a.reps, batch_count=a.batches, verbose=True)
     with open(a.out, "w") as f:
         json.dump(db, f)
-    print(f"{len(db)} records -> {a.out}; all variants agree: {all(r['agree'] for r in db)}")
+    print(f"{len(db)} records -> {a.out}; all configurations agree: {all(r['agree'] for r in db)}")
 
 
 if __name__ == "__main__":

@@ -30,7 +30,7 @@ MEXOUT = os.path.join(MEXDIR, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-              "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
+              "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE, "-I" + OBJ]
 GATEWAYS = ("mela_matmul_gf2", "mela_matmul_m4ri", "mela_rank_gf2", "mela_rank_m4ri",
             "mela_null_gf2", "mela_null_m4ri")
 
@@ -69,10 +69,42 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+MODEL_JSON = os.path.join(PKG, "costmodel.json")
+MODEL_INC = os.path.join(OBJ, "costmodel_weights.inc")
+
+
+def write_model_weights() -> None:
+    """The trained cost model (costmodel.json) as a C initializer list that
+    mlp.cu compiles in as the library's default dispatch model.  Without a
+    model file of the network's size the include is empty and the library
+    starts on its fixed rule."""
+    import json
+    import re
+    params = []
+    if os.path.exists(MODEL_JSON):
+        with open(os.path.join(INCLUDE, "mela.h")) as f:
+            want = int(re.search(r"#define MELA_MLP_PARAMS (\d+)", f.read()).group(1))
+        with open(MODEL_JSON) as f:
+            p = json.load(f)["params"]
+        if len(p) == want:
+            params = p
+    text = "// generated from costmodel.json by build.py\n"
+    if params:
+        text += "#define MELA_DEFAULT_MODEL 1\n"
+        text += "static const float kDefaultModel[] = {\n"
+        text += ",\n".join(", ".join(f"{float(x)!r}f" for x in params[i:i + 8]) for i in range(0, len(params), 8))
+        text += "\n};\n"
+    old = open(MODEL_INC).read() if os.path.exists(MODEL_INC) else None
+    if old != text:
+        with open(MODEL_INC, "w") as f:
+            f.write(text)
+
+
 def build_library(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
+    write_model_weights()
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    hdrs = _headers()
+    hdrs = _headers() + [MODEL_INC]
     jobs = []
     for src in sources:
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")

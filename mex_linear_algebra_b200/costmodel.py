@@ -2,17 +2,24 @@
 
 Training runs entirely in the library's kernels (mela_mlp_gradient +
 mela_mlp_adam_step, full-batch Adam); torch only holds the buffers.  The
-model predicts log2(microseconds) for each of a request's variants;
-``choose`` returns the variant with the smallest prediction, and
-``install`` hands the weights to the library's dispatcher.  Without an
-installed model the library uses its fixed rule.
+model predicts log2(microseconds) for each configuration of a request -- a
+variant with its tuning fields (Four-Russians k, tile), or for a matrix in a
+batched launch the engine that runs it; ``choose`` returns the configuration
+with the smallest prediction, and ``install`` hands the weights to the
+library's dispatcher (the library also installs costmodel.json by itself
+when it is built with one).  Without an installed model the library uses its
+fixed rule.
 
-Timing databases come from :mod:`mex_linear_algebra_b200.autotune`.
+Inputs per request: shape, density, the op, and the batch mix (how many
+matrices share the launch and their mean log2(m*n); 1 and the request's own
+size for single calls).  Timing databases come from
+:mod:`mex_linear_algebra_b200.autotune`.
 """
 from __future__ import annotations
 
 import ctypes as C
 import json
+import math
 import os
 
 import numpy as np
@@ -22,25 +29,56 @@ from ._lib import check, lib
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(PKG, "costmodel.json")
-OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL}
-VARIANT_NAMES = {"matmul": ("plain", "m4ri", "tc", "tc_fp4"),
-                 "rank": ("plain", "m4ri", "m4ri_k4", "fused", "tc"),
-                 "null": ("plain", "m4ri", "m4ri_k4", "fused", "tc")}
+OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL, "batch": _lib.OP_BATCH}
+
+# Configuration names in the model's output order (dispatch.cu lists the
+# variant arguments; config_codes() reads them from the library).
+ELIM_CONFIGS = ("plain", "m4ri_k4", "m4ri_k6", "m4ri_k7", "m4ri_k8", "m4ri_k8_rt256", "m4ri_k9_rt4096",
+                "m4ri_k10_rt4096", "fused", "tc")
+CONFIG_NAMES = {"rank": ELIM_CONFIGS, "null": ELIM_CONFIGS,
+                "matmul": ("plain", "m4ri", "tc_pair", "tc_single", "tc_fp4_pair", "tc_fp4_single"),
+                "batch": ("cta", "group", "warp")}
+# kept for callers of the earlier name
+VARIANT_NAMES = CONFIG_NAMES
 
 
-def features(op: str, m: int, n: int, p: int, density: float) -> np.ndarray:
+def config_codes(op: str) -> tuple:
+    """Variant arguments of the op's configurations, from the library."""
+    L = lib()
+    n = L.mela_costmodel_config_count(OPS[op])
+    return tuple(int(L.mela_costmodel_config(OPS[op], i)) for i in range(n))
+
+
+def config_code(op: str, name: str) -> int:
+    return config_codes(op)[CONFIG_NAMES[op].index(name)]
+
+
+def _mix(m, n, batch_log2_cells):
+    if batch_log2_cells is not None:
+        return float(batch_log2_cells)
+    return math.log2(max(float(m) * float(n), 1.0))
+
+
+def features(op: str, m: int, n: int, p: int, density: float, batch_count: int = 1,
+             batch_log2_cells: float | None = None) -> np.ndarray:
     x = (C.c_float * _lib.MLP_IN)()
-    lib().mela_costmodel_features(OPS[op], int(m), int(n), int(p), float(density), x)
+    lib().mela_costmodel_features(OPS[op], int(m), int(n), int(p), float(density), int(batch_count),
+                                  _mix(m, n, batch_log2_cells), x)
     return np.array(list(x), dtype=np.float32)
 
 
+def record_features(r) -> np.ndarray:
+    return features(r["op"], r["m"], r["n"], r.get("p", 0), r["density"], r.get("batch_count", 1),
+                    r.get("batch_log2_cells"))
+
+
 def dataset(records):
-    """Records (autotune DB rows) -> X (N x 8), T (N x 5 log2 us), mask (N x 5)."""
-    X = np.stack([features(r["op"], r["m"], r["n"], r.get("p", 0), r["density"]) for r in records])
+    """Records (autotune DB rows) -> X (N x IN), T (N x OUT log2 us), mask (N x OUT)."""
+    X = np.stack([record_features(r) for r in records]) if records else np.zeros((0, _lib.MLP_IN), np.float32)
     T = np.zeros((len(records), _lib.MLP_OUT), dtype=np.float32)
     Mk = np.zeros_like(T)
     for i, r in enumerate(records):
-        for v, name in enumerate(VARIANT_NAMES[r["op"]]):
+        for v, name in enumerate(CONFIG_NAMES[r["op"]]):
             t = r["times_us"].get(name)
             if t is not None and t > 0:
                 T[i, v] = np.log2(t)
@@ -75,7 +113,6 @@ def train(records, steps: int = 3000, lr: float = 3e-3, seed: int = 0, log_every
     inv = 1.0 / max(float(Mk.sum()), 1.0)
     s = torch.cuda.current_stream().cuda_stream
     L = lib()
-    last = None
     for step in range(1, steps + 1):
         check(L.mela_mlp_gradient(P.data_ptr(), dX.data_ptr(), dT.data_ptr(), dM.data_ptr(), len(X),
                                   inv, G.data_ptr(), loss.data_ptr(), s))
@@ -103,7 +140,10 @@ def save(params: np.ndarray, path: str = DEFAULT_MODEL, meta: dict | None = None
 
 def load(path: str = DEFAULT_MODEL) -> np.ndarray:
     with open(path) as f:
-        return np.array(json.load(f)["params"], dtype=np.float32)
+        p = np.array(json.load(f)["params"], dtype=np.float32)
+    if p.size != _lib.MLP_PARAMS:
+        raise ValueError(f"{path}: {p.size} parameters, the library's network has {_lib.MLP_PARAMS}")
+    return p
 
 
 def install(params: np.ndarray | None):
@@ -117,46 +157,55 @@ def install(params: np.ndarray | None):
     check(lib().mela_costmodel_load(buf.ctypes.data))
 
 
-def choose(op: str, m: int, n: int, p: int, density: float) -> str:
-    """Variant the installed model picks (name); the fixed rule without one."""
-    v = lib().mela_costmodel_choose(OPS[op], int(m), int(n), int(p), float(density))
+def choose(op: str, m: int, n: int, p: int, density: float, batch_count: int = 1,
+           batch_log2_cells: float | None = None) -> str:
+    """Configuration the installed model picks (name); the fixed rule without one."""
+    v = lib().mela_costmodel_choose(OPS[op], int(m), int(n), int(p), float(density), int(batch_count),
+                                    _mix(m, n, batch_log2_cells))
     if v < 0:
         return heuristic(op, m, n, p, density)
-    return VARIANT_NAMES[op][v]
+    return CONFIG_NAMES[op][v]
 
 
-def heuristic(op: str, m: int, n: int, p: int, density: float) -> str:
-    """The library's fixed rule (what dispatch does without a model)."""
+def heuristic(op: str, m: int, n: int, p: int, density: float, rule: str | None = None) -> str:
+    """The library's fixed rule (what dispatch does without a model).  For
+    batch records the rule's engine depends on shared-memory fit, which the
+    autotuner records with each request (``rule``)."""
+    if op == "batch":
+        return rule or "cta"
     if op == "matmul":
         if m >= 1024 and n >= 1024 and p >= 1024:
-            return "tc_fp4" if n < (1 << 23) else "tc"
+            return "tc_fp4_pair" if n < (1 << 23) else "tc_pair"
         return "plain"
     return "fused" if m * n < 8192 else "tc"
 
 
 def evaluate(params: np.ndarray, records):
     """Measured cost of the model's choices vs the exhaustive best and vs the
-    fixed rule, on records with every variant timed: totals (dominated by the
-    largest requests) and per-request means of time/best - 1."""
+    fixed rule, on records with every feasible configuration timed: totals
+    (dominated by the largest requests) and per-request means of
+    time/best - 1."""
     X, T, Mk = dataset(records)
     Y = predict(params, X) if len(X) else np.zeros((0, _lib.MLP_OUT))
     tot_best = tot_model = tot_rule = 0.0
     reg_model, reg_rule = [], []
     agree = used = 0
     for i, r in enumerate(records):
-        names = VARIANT_NAMES[r["op"]]
+        names = CONFIG_NAMES[r["op"]]
         times = [r["times_us"].get(nm) for nm in names]
-        if any(t is None for t in times):
+        feasible = [j for j, t in enumerate(times) if t is not None]
+        rule_name = heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"], r.get("rule"))
+        if not feasible or rule_name not in r["times_us"]:
             continue
         used += 1
-        best = min(times)
-        pred = int(np.argmin(np.where(Mk[i, :len(names)] > 0, Y[i, :len(names)], np.inf)))
-        rule = names.index(heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"]))
+        best = min(times[j] for j in feasible)
+        pred = feasible[int(np.argmin([Y[i, j] for j in feasible]))]
+        t_rule = r["times_us"][rule_name]
         tot_best += best
         tot_model += times[pred]
-        tot_rule += times[rule]
+        tot_rule += t_rule
         reg_model.append(times[pred] / best - 1.0)
-        reg_rule.append(times[rule] / best - 1.0)
+        reg_rule.append(t_rule / best - 1.0)
         agree += int(times[pred] == best)
     return {"records": used, "total_best_us": tot_best, "total_model_us": tot_model,
             "total_rule_us": tot_rule,

@@ -182,7 +182,8 @@ static i64 round_up(i64 x, i64 a) { return (x + a - 1) / a * a; }
 
 // workspace layout for each variant
 struct GemmPlan {
-    int variant;
+    int variant;          // base variant
+    int tc_tile;          // tensor-core tile choice (0 default, 1 single CTAs, 2 CTA pairs)
     i64 ldbt;             // packed Bt row pitch (words)
     size_t bt_bytes;      // packed Bt
     i64 mp, np, kp;       // padded byte-operand shape (tensor cores)
@@ -190,38 +191,24 @@ struct GemmPlan {
     size_t total;
 };
 
-int choose_gemm_variant(i64 m, i64 k, i64 n)
-{
-    // the learned cost model when one is installed (dense input assumed)
-    const int c = costmodel_choose(MELA_OP_MATMUL, (double)m, (double)k, (double)n, 0.5);
-    if (c >= 0) {
-        static const int order[4] = {MELA_GEMM_PLAIN, MELA_GEMM_M4RI, MELA_GEMM_TC, MELA_GEMM_TC_FP4};
-        const int v = order[c & 3];
-        if (v == MELA_GEMM_TC_FP4 && k >= (1LL << 23)) return MELA_GEMM_TC;
-        return v;
-    }
-    // fixed rule: tensor cores pay off once every dimension spans a few
-    // tiles (below that the expansion of the operands dominates); the FP4
-    // form runs at twice the INT8 rate while its f32 sums stay exact
-    if (m >= 1024 && n >= 1024 && k >= 1024) return k < (1LL << 23) ? MELA_GEMM_TC_FP4 : MELA_GEMM_TC;
-    return MELA_GEMM_PLAIN;
-}
-
-static GemmPlan plan_gemm(int variant, i64 m, i64 k, i64 n)
+// Workspace layout of a concrete variant argument (AUTO already resolved).
+static GemmPlan plan_gemm(int32_t variant, i64 m, i64 k, i64 n)
 {
     GemmPlan p{};
-    if (variant == MELA_GEMM_AUTO) variant = choose_gemm_variant(m, k, n);
-    p.variant = variant;
+    Tuning t{};
+    if (!decode_gemm_variant(variant, &t) || t.base == MELA_GEMM_AUTO) t.base = MELA_GEMM_PLAIN;
+    p.variant = t.base;
+    p.tc_tile = t.tc_tile;
     p.ldbt = even_words(k);
-    if (variant == MELA_GEMM_PLAIN) p.bt_bytes = (size_t)n * p.ldbt * 8;
-    if (variant == MELA_GEMM_TC) {
+    if (p.variant == MELA_GEMM_PLAIN) p.bt_bytes = (size_t)n * p.ldbt * 8;
+    if (p.variant == MELA_GEMM_TC) {
         p.mp = round_up(m, 256);  // 256-row tiles for CTA pairs
         p.np = round_up(n, 256);
         p.kp = round_up(k, 128);  // bytes = values
         p.a8_bytes = (size_t)p.mp * p.kp;
         p.b8_bytes = (size_t)p.np * p.kp;
     }
-    if (variant == MELA_GEMM_TC_FP4) {
+    if (p.variant == MELA_GEMM_TC_FP4) {
         p.mp = round_up(m, 256);
         p.np = round_up(n, 256);
         p.kp = round_up(k, 256) / 2;  // bytes, two values each
@@ -264,6 +251,7 @@ mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 l
                          i64 n, void *ws, size_t ws_bytes, cudaStream_t s)
 {
     if (m == 0 || n == 0 || k == 0) return MELA_OK;
+    variant = resolve_gemm_variant(variant, A, lda, m, k, n, s);
     GemmPlan p = plan_gemm(variant, m, k, n);
     mela_status st = check_ws(p, ws, ws_bytes);
     if (st != MELA_OK) return st;
@@ -299,19 +287,20 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
         MELA_CUDA_TRY(cudaMemset2DAsync(C, (size_t)ldc * 8, 0, (size_t)words_of(n) * 8, (size_t)m, s));
         return MELA_OK;
     }
+    variant = resolve_gemm_variant(variant, A, lda, m, k, n, s);
     GemmPlan p = plan_gemm(variant, m, k, n);
     mela_status st = check_ws(p, ws, ws_bytes);
     if (st != MELA_OK) return st;
     GemmBufs b = carve(p, ws);
     switch (p.variant) {
     case MELA_GEMM_PLAIN: return launch_gemm_plain(A, lda, b.Bt, p.ldbt, C, ldc, m, k, n, s);
-    case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, false);
+    case MELA_GEMM_TC: return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, false, p.tc_tile);
     case MELA_GEMM_TC_FP4:
         if (k >= (1LL << 23)) {
             set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
             return MELA_ERR_UNSUPPORTED;
         }
-        return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, true);
+        return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, true, p.tc_tile);
     case MELA_GEMM_M4RI: return launch_gemm_m4ri(A, lda, B, ldb, C, ldc, m, k, n, s);
     default:
         set_error("unknown product variant %d", p.variant);
@@ -322,6 +311,7 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
 mela_status gemm_device(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                         i64 m, i64 k, i64 n, void *ws, size_t ws_bytes, cudaStream_t s)
 {
+    if (m > 0 && n > 0 && k > 0) variant = resolve_gemm_variant(variant, A, lda, m, k, n, s);
     mela_status st = gemm_prepare(variant, A, lda, B, ldb, m, k, n, ws, ws_bytes, s);
     if (st != MELA_OK) return st;
     return gemm_run(variant, A, lda, B, ldb, C, ldc, m, k, n, ws, ws_bytes, s);
@@ -330,7 +320,14 @@ mela_status gemm_device(int variant, const u64 *A, i64 lda, const u64 *B, i64 ld
 size_t gemm_workspace(int variant, i64 m, i64 k, i64 n)
 {
     if (m <= 0 || n <= 0 || k <= 0) return 0;
-    return plan_gemm(variant, m, k, n).total;
+    if (MELA_VARIANT_BASE(variant) != MELA_GEMM_AUTO) return plan_gemm(variant, m, k, n).total;
+    // AUTO decides on the data: room for any configuration it may pick
+    size_t most = plan_gemm(fixed_gemm_variant(m, k, n), m, k, n).total;
+    for (int c = 0; c < config_count(MELA_OP_MATMUL); ++c) {
+        const size_t t = plan_gemm(config_variant(MELA_OP_MATMUL, c), m, k, n).total;
+        if (t > most) most = t;
+    }
+    return most;
 }
 
 // ---------------------------------------------------------------- host-matrix helpers
@@ -392,7 +389,8 @@ extern "C" mela_status mela_device_error_flags(uint32_t *flags, int clear)
 
 extern "C" size_t mela_matmul_workspace_size(int32_t variant, int64_t m, int64_t k, int64_t n)
 {
-    if (variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4) return 0;
+    Tuning t;
+    if (!decode_gemm_variant(variant, &t)) return 0;
     return gemm_workspace(variant, m, k, n);
 }
 
@@ -401,7 +399,8 @@ extern "C" mela_status mela_dev_matmul(int32_t variant, const uint64_t *dA, int6
                                        int64_t m, int64_t k, int64_t n, void *workspace,
                                        size_t workspace_bytes, void *stream)
 {
-    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4 ||
+    Tuning tn;
+    if (m < 0 || k < 0 || n < 0 || !decode_gemm_variant(variant, &tn) ||
         lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
         set_error("mela_dev_matmul: bad shape, leading dimension or variant");
         return MELA_ERR_INVALID;
@@ -418,7 +417,8 @@ static mela_status check_dev_matmul_args(int32_t variant, const uint64_t *dA, in
                                          const uint64_t *dB, int64_t ldb, int64_t ldc, int64_t m,
                                          int64_t k, int64_t n)
 {
-    if (m < 0 || k < 0 || n < 0 || variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4 ||
+    Tuning tn;
+    if (m < 0 || k < 0 || n < 0 || !decode_gemm_variant(variant, &tn) ||
         lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n)) {
         set_error("bad shape, leading dimension or variant");
         return MELA_ERR_INVALID;
@@ -475,7 +475,7 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
     cudaStream_t sin = nullptr, sout = nullptr;
     mela_status st = copy_streams(&sin, &sout);
     if (st != MELA_OK) return st;
-    const bool fp4 = variant == MELA_GEMM_TC_FP4;
+    const bool fp4 = MELA_VARIANT_BASE(variant) == MELA_GEMM_TC_FP4;
     if (fp4 && k >= (1LL << 23)) {
         set_error("fp4 tensor-core product needs k < 2^23 (exact f32 sums)");
         return MELA_ERR_UNSUPPORTED;
@@ -518,7 +518,8 @@ static mela_status matmul_packed_host_pipelined(const uint64_t *A, int64_t lda, 
     auto product = [&](int i, int j) -> mela_status {
         const i64 r0 = i * mb, c0 = j * nb, rows = rows_of(i), cols = cols_of(j);
         mela_status e = launch_gemm_tc(b.A8 + (size_t)r0 * p.kp, b.B8 + (size_t)c0 * p.kp, round_up(rows, 256),
-                                       round_up(cols, 256), p.kp, c + r0 * wn + c0 / 64, wn, rows, cols, s, fp4);
+                                       round_up(cols, 256), p.kp, c + r0 * wn + c0 / 64, wn, rows, cols, s, fp4,
+                                       p.tc_tile);
         if (e != MELA_OK) return e;
         MELA_CUDA_TRY(cudaEventRecord(ev_c(i, j), s));
         MELA_CUDA_TRY(cudaStreamWaitEvent(sout, ev_c(i, j), 0));
@@ -584,8 +585,9 @@ extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, c
                                                int64_t ldb, uint64_t *C, int64_t ldc, int64_t m,
                                                int64_t k, int64_t n, int32_t variant)
 {
+    Tuning tn;
     if (m < 0 || k < 0 || n < 0 || lda < words_of(k) || ldb < words_of(n) || ldc < words_of(n) ||
-        variant < MELA_GEMM_AUTO || variant > MELA_GEMM_TC_FP4) {
+        !decode_gemm_variant(variant, &tn)) {
         set_error("mela_matmul_packed_host: bad shape or variant");
         return MELA_ERR_INVALID;
     }
@@ -594,8 +596,13 @@ extern "C" mela_status mela_matmul_packed_host(const uint64_t *A, int64_t lda, c
     mela_status st = host_stream(&s);
     if (st != MELA_OK) return st;
     {
-        const int v = plan_gemm(variant, m, k, n).variant;
-        if ((v == MELA_GEMM_TC || v == MELA_GEMM_TC_FP4) && k > 0 && m >= kPipeMin && n >= kPipeMin)
+        // The transfers are pipelined for an explicit tensor-core variant, and
+        // for AUTO under the fixed rule; AUTO with a cost model installed
+        // uploads first, since the model's choice depends on the data.
+        int32_t v = variant;
+        if (tn.base == MELA_GEMM_AUTO && !costmodel_loaded()) v = fixed_gemm_variant(m, k, n);
+        const int b = MELA_VARIANT_BASE(v);
+        if ((b == MELA_GEMM_TC || b == MELA_GEMM_TC_FP4) && k > 0 && m >= kPipeMin && n >= kPipeMin)
             return matmul_packed_host_pipelined(A, lda, B, ldb, C, ldc, m, k, n, v, s);
     }
     const i64 wk = words_of(k), wn = words_of(n);

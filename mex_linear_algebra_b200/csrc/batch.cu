@@ -26,6 +26,7 @@
 // directly: Zt row i = e_{f_i} + sum_p RREF(p, f_i) e_{piv(p)}.
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -1028,13 +1029,27 @@ static mela_status plan_free(BatchPlanImpl *P)
     return MELA_OK;
 }
 
+// Engine per matrix.  policy -1: by fit and size (the fixed rule below);
+// 0/1/2: that engine wherever the matrix fits its region; -2: the installed
+// cost model's cheapest engine among those the matrix fits, given its shape,
+// its density and the batch mix (matrix count, mean log2(m*n)) -- the fixed
+// rule when no model is installed.
 static mela_status plan_create(const mela_batch_item *h, long long count, int force_class,
-                               BatchPlanImpl **out)
+                               const double *densities, BatchPlanImpl **out)
 {
     *out = nullptr;
     if (count < 0 || (count > 0 && !h) || count > INT_MAX) {
         set_error("batch: bad item list");
         return MELA_ERR_INVALID;
+    }
+    const bool learned = force_class == -2 && costmodel_loaded();
+    double mix = 0.0;
+    if (learned) {
+        for (long long i = 0; i < count; ++i) {
+            const double cells = (double)h[i].m * (double)h[i].n;
+            mix += std::log2(cells > 1 ? cells : 1);
+        }
+        mix /= (double)(count ? count : 1);
     }
     BatchPlanImpl *P = new BatchPlanImpl();
     P->count = (int)count;
@@ -1068,6 +1083,14 @@ static mela_status plan_create(const mela_batch_item *h, long long count, int fo
             // a forced class must still fit its region; otherwise fall back to big
             const size_t budget = force_class == 2 ? kSmallBudget : force_class == 1 ? kMidBudget : kSmemTotal;
             if (force_class == 0 || aux + mat <= budget) c = force_class;
+        } else if (learned) {
+            float y[MELA_MLP_OUT];
+            const double dens = densities ? densities[i] : 0.5;
+            if (costmodel_predict(MELA_OP_BATCH, (double)m, (double)n, 0.0, dens, (double)count, mix, y)) {
+                c = 0;
+                if (aux + mat <= (size_t)kMidBudget && y[1] < y[c]) c = 1;
+                if (aux + mat <= (size_t)kSmallBudget && y[2] < y[c]) c = 2;
+            }
         }
         if (c == 0) {
             d.flags = 0;  // big matrices live in the CTA's global scratch
@@ -1232,16 +1255,76 @@ struct mela_batch_plan {
 extern "C" mela_status mela_batch_plan_create(const mela_batch_item *items, int64_t count,
                                               int32_t force_class, mela_batch_plan **plan)
 {
+    return mela_batch_plan_create_ex(items, count, nullptr, force_class, plan);
+}
+
+extern "C" mela_status mela_batch_plan_create_ex(const mela_batch_item *items, int64_t count,
+                                                 const double *densities, int32_t policy,
+                                                 mela_batch_plan **plan)
+{
     if (!plan) {
         set_error("null plan pointer");
         return MELA_ERR_INVALID;
     }
     *plan = nullptr;
+    if (policy < -2 || policy > 2) {
+        set_error("batch: engine policy %d (-2 .. 2)", policy);
+        return MELA_ERR_INVALID;
+    }
     BatchPlanImpl *P = nullptr;
-    mela_status st = plan_create(items, count, force_class, &P);
+    mela_status st = plan_create(items, count, policy, densities, &P);
     if (st != MELA_OK) return st;
     *plan = new mela_batch_plan{P};
     return MELA_OK;
+}
+
+namespace mela {
+// d_counts[i] += ones of item i (one CTA per item, grid-stride over items).
+static __global__ void __launch_bounds__(256)
+batch_popcount_kernel(const mela_batch_item *items, long long count, const u64 *in, long long *counts)
+{
+    for (long long i = blockIdx.x; i < count; i += gridDim.x) {
+        const mela_batch_item it = items[i];
+        const long long wc = (it.n + 63) / 64, total = it.m * wc;
+        const u64 last = (it.n & 63) ? ((1ull << (it.n & 63)) - 1) : ~0ull;
+        unsigned long long c = 0;
+        for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+            u64 v = in[it.in_offset + e];
+            if (e % wc == wc - 1) v &= last;
+            c += __popcll(v);
+        }
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd((unsigned long long *)&counts[i], c);
+    }
+}
+}  // namespace mela
+
+extern "C" mela_status mela_batch_popcounts(const mela_batch_item *items, int64_t count, const uint64_t *d_in,
+                                            int64_t *d_counts, void *stream)
+{
+    if (count < 0 || (count > 0 && (!items || !d_in || !d_counts))) {
+        set_error("mela_batch_popcounts: bad arguments");
+        return MELA_ERR_INVALID;
+    }
+    if (count == 0) return MELA_OK;
+    for (int64_t i = 0; i < count; ++i) {
+        if (items[i].m < 0 || items[i].n < 0 || items[i].in_offset < 0) {
+            set_error("mela_batch_popcounts: item %lld has a bad shape or offset", (long long)i);
+            return MELA_ERR_INVALID;
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf d_items;
+    mela_status st = d_items.alloc((size_t)count * sizeof(mela_batch_item), s);
+    if (st != MELA_OK) return st;
+    MELA_CUDA_TRY(cudaMemcpyAsync(d_items.p, items, (size_t)count * sizeof(mela_batch_item),
+                                  cudaMemcpyHostToDevice, s));
+    MELA_CUDA_TRY(cudaMemsetAsync(d_counts, 0, (size_t)count * 8, s));
+    const long long grid = count < (long long)sm_count() * 16 ? count : (long long)sm_count() * 16;
+    batch_popcount_kernel<<<(unsigned)grid, 256, 0, s>>>((const mela_batch_item *)d_items.p, count,
+                                                         (const u64 *)d_in, (long long *)d_counts);
+    MELA_LAUNCH_CHECK("batch_popcount_kernel");
+    return MELA_OK;  // the item copy is released on s, after the kernel
 }
 
 extern "C" void mela_batch_plan_destroy(mela_batch_plan *plan)

@@ -1,0 +1,242 @@
+// dispatch.cu -- how each request is computed: variant arguments with their
+// tuning fields, the configurations the cost model prices, the density it is
+// fed, and the fixed rule it is compared against.
+//
+// A variant argument is a base variant (bits 0-7) with optional tuning
+// fields (MELA_TUNE_K, MELA_TUNE_TILE in include/mela.h).  The AUTO
+// variants ask the installed cost model for a configuration -- measuring
+// the input's density on the device first -- or, without a model, apply
+// the fixed rule.  Nothing here changes a result.
+#include <cmath>
+
+#include "mela_common.cuh"
+#include "mela_internal.h"
+#include "mela_host.h"
+
+namespace mela {
+
+// ---------------------------------------------------------------- variant arguments
+bool decode_elim_variant(int32_t v, Tuning *t)
+{
+    if (v & ~0xffff) return false;
+    const int base = v & 0xff, k = (v >> 8) & 0xf, tile = (v >> 12) & 0xf;
+    if (base < MELA_ELIM_AUTO || base > MELA_ELIM_TC) return false;
+    Tuning r{};
+    r.base = base;
+    r.k = 0;
+    r.row_tile = 1024;
+    r.tc_tile = 0;
+    if (base == MELA_ELIM_M4RI || base == MELA_ELIM_M4RI_K4) {
+        const int dflt = base == MELA_ELIM_M4RI ? 8 : 4;
+        r.k = k ? k : dflt;
+        if (base == MELA_ELIM_M4RI_K4 && r.k != 4) return false;
+        if (r.k != 4 && (r.k < 6 || r.k > 10)) return false;
+        static const int tiles[4] = {1024, 256, 1024, 4096};
+        if (tile > 3) return false;
+        r.row_tile = tiles[tile];
+    } else if (k || tile) {
+        return false;
+    }
+    *t = r;
+    return true;
+}
+
+bool decode_gemm_variant(int32_t v, Tuning *t)
+{
+    if (v & ~0xffff) return false;
+    const int base = v & 0xff, k = (v >> 8) & 0xf, tile = (v >> 12) & 0xf;
+    if (base < MELA_GEMM_AUTO || base > MELA_GEMM_TC_FP4) return false;
+    Tuning r{};
+    r.base = base;
+    r.row_tile = 0;
+    r.k = 0;
+    r.tc_tile = 0;
+    if (base == MELA_GEMM_M4RI) {
+        if (k && k != 8) return false;
+        r.k = 8;
+        if (tile) return false;
+    } else if (base == MELA_GEMM_TC || base == MELA_GEMM_TC_FP4) {
+        if (k || tile > 2) return false;
+        r.tc_tile = tile;
+    } else if (k || tile) {
+        return false;
+    }
+    *t = r;
+    return true;
+}
+
+// ---------------------------------------------------------------- configurations
+// Model output order per op.  Elimination: the plain form, the blocked form
+// over M4RI k = 4, 6, 7, 8 (with 1024-row update tiles), k = 8 with 256-row
+// tiles (more CTAs for short matrices), k = 9 and 10 with 4096-row tiles
+// (their larger tables pay off over more rows), the single-CTA form and the
+// tensor-core windows.  Products: plain, Four-Russians, and each tensor-core
+// form on CTA pairs and on single CTAs.  Batches: the engine per matrix.
+static const int32_t kElimConfigs[] = {
+    MELA_ELIM_PLAIN,
+    MELA_ELIM_M4RI_K4,
+    MELA_ELIM_M4RI | MELA_TUNE_K(6),
+    MELA_ELIM_M4RI | MELA_TUNE_K(7),
+    MELA_ELIM_M4RI | MELA_TUNE_K(8),
+    MELA_ELIM_M4RI | MELA_TUNE_K(8) | MELA_TUNE_TILE(1),
+    MELA_ELIM_M4RI | MELA_TUNE_K(9) | MELA_TUNE_TILE(3),
+    MELA_ELIM_M4RI | MELA_TUNE_K(10) | MELA_TUNE_TILE(3),
+    MELA_ELIM_FUSED,
+    MELA_ELIM_TC,
+};
+static const int32_t kGemmConfigs[] = {
+    MELA_GEMM_PLAIN,
+    MELA_GEMM_M4RI,
+    MELA_GEMM_TC | MELA_TUNE_TILE(2),
+    MELA_GEMM_TC | MELA_TUNE_TILE(1),
+    MELA_GEMM_TC_FP4 | MELA_TUNE_TILE(2),
+    MELA_GEMM_TC_FP4 | MELA_TUNE_TILE(1),
+};
+static const int32_t kBatchConfigs[] = {0, 1, 2};
+static_assert(sizeof kElimConfigs / sizeof kElimConfigs[0] <= MELA_MLP_OUT, "model outputs");
+static_assert(sizeof kGemmConfigs / sizeof kGemmConfigs[0] <= MELA_MLP_OUT, "model outputs");
+
+int config_count(int op)
+{
+    switch (op) {
+    case MELA_OP_RANK:
+    case MELA_OP_NULL: return (int)(sizeof kElimConfigs / sizeof kElimConfigs[0]);
+    case MELA_OP_MATMUL: return (int)(sizeof kGemmConfigs / sizeof kGemmConfigs[0]);
+    case MELA_OP_BATCH: return (int)(sizeof kBatchConfigs / sizeof kBatchConfigs[0]);
+    default: return 0;
+    }
+}
+
+int32_t config_variant(int op, int index)
+{
+    if (index < 0 || index >= config_count(op)) return -1;
+    switch (op) {
+    case MELA_OP_RANK:
+    case MELA_OP_NULL: return kElimConfigs[index];
+    case MELA_OP_MATMUL: return kGemmConfigs[index];
+    default: return kBatchConfigs[index];
+    }
+}
+
+// ---------------------------------------------------------------- density
+namespace {
+__global__ void popcount_kernel(const u64 *__restrict__ M, i64 ld, i64 m, i64 wc, u64 last_mask,
+                                unsigned long long *count)
+{
+    unsigned long long c = 0;
+    const i64 total = m * wc;
+    for (i64 e = blockIdx.x * (i64)blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
+        const i64 i = e / wc, w = e - i * wc;
+        u64 v = M[i * ld + w];
+        if (w == wc - 1) v &= last_mask;
+        c += __popcll(v);
+    }
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ unsigned long long part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += part[q];
+        atomicAdd(count, t);
+    }
+}
+}  // namespace
+
+mela_status launch_popcount(const u64 *M, i64 ld, i64 m, i64 n, long long *d_count, cudaStream_t s)
+{
+    MELA_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(long long), s));
+    if (m <= 0 || n <= 0) return MELA_OK;
+    const i64 wc = words_of(n);
+    const u64 last_mask = (n & 63) ? ((1ull << (n & 63)) - 1) : ~0ull;
+    i64 blocks = (m * wc + 255) / 256;
+    const i64 cap = (i64)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    popcount_kernel<<<(unsigned)blocks, 256, 0, s>>>(M, ld, m, wc, last_mask, (unsigned long long *)d_count);
+    MELA_LAUNCH_CHECK("popcount_kernel");
+    return MELA_OK;
+}
+
+double measure_density(const u64 *M, i64 ld, i64 m, i64 n, cudaStream_t s)
+{
+    if (m <= 0 || n <= 0 || !M) return 0.5;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return 0.5;  // no read-back while a graph is being captured
+    }
+    DevBuf cnt;
+    if (cnt.alloc(sizeof(long long), s) != MELA_OK) return 0.5;
+    long long h = 0;
+    if (launch_popcount(M, ld, m, n, (long long *)cnt.p, s) != MELA_OK ||
+        cudaMemcpyAsync(&h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.5;
+    }
+    return (double)h / ((double)m * (double)n);
+}
+
+// ---------------------------------------------------------------- choices
+int32_t resolve_gemm_variant(int32_t variant, const u64 *A, i64 lda, i64 m, i64 k, i64 n, cudaStream_t s)
+{
+    if (MELA_VARIANT_BASE(variant) != MELA_GEMM_AUTO) return variant;
+    if (costmodel_loaded() && m > 0 && n > 0 && k > 0) {
+        const double d = measure_density(A, lda, m, k, s);
+        const int c = costmodel_choose(MELA_OP_MATMUL, (double)m, (double)k, (double)n, d, 1,
+                                       std::log2((double)m * (double)k));
+        if (c >= 0) {
+            int32_t v = config_variant(MELA_OP_MATMUL, c);
+            // the FP4 form's f32 sums are exact below 2^24: past 2^23 terms use INT8
+            if (MELA_VARIANT_BASE(v) == MELA_GEMM_TC_FP4 && k >= (1LL << 23))
+                v = MELA_GEMM_TC | (v & ~0xff);
+            return v;
+        }
+    }
+    return fixed_gemm_variant(m, k, n);
+}
+
+int32_t fixed_gemm_variant(i64 m, i64 k, i64 n)
+{
+    // tensor cores pay off once every dimension spans a few tiles (below
+    // that the expansion of the operands dominates); the FP4 form runs at
+    // twice the INT8 rate while its f32 sums stay exact
+    if (m >= 1024 && n >= 1024 && k >= 1024) return k < (1LL << 23) ? MELA_GEMM_TC_FP4 : MELA_GEMM_TC;
+    return MELA_GEMM_PLAIN;
+}
+
+int32_t resolve_elim_variant(int32_t variant, const u64 *M, i64 ld, i64 m, i64 n, int rref, cudaStream_t s)
+{
+    if (MELA_VARIANT_BASE(variant) != MELA_ELIM_AUTO) return variant;
+    if (costmodel_loaded() && m > 0 && n > 0) {
+        const double d = measure_density(M, ld, m, n, s);
+        const int c = costmodel_choose(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0, d, 1,
+                                       std::log2((double)m * (double)n));
+        if (c >= 0) return config_variant(MELA_OP_RANK, c);
+    }
+    return fixed_elim_variant(m, n);
+}
+
+int32_t fixed_elim_variant(i64 m, i64 n)
+{
+    // one CTA for small matrices, tensor-core windows otherwise
+    return (double)m * (double)n < 8192.0 ? MELA_ELIM_FUSED : MELA_ELIM_TC;
+}
+
+}  // namespace mela
+
+using namespace mela;
+
+extern "C" int32_t mela_costmodel_config_count(int32_t op) { return config_count(op); }
+
+extern "C" int32_t mela_costmodel_config(int32_t op, int32_t index) { return config_variant(op, index); }
+
+extern "C" mela_status mela_dev_popcount(const uint64_t *dM, int64_t ld, int64_t m, int64_t n, int64_t *d_count,
+                                         void *stream)
+{
+    if (m < 0 || n < 0 || !d_count || (m > 0 && n > 0 && (!dM || ld < words_of(n)))) {
+        set_error("mela_dev_popcount: bad shape, leading dimension or pointer");
+        return MELA_ERR_INVALID;
+    }
+    return launch_popcount((const u64 *)dM, ld, m, n, (long long *)d_count, (cudaStream_t)stream);
+}

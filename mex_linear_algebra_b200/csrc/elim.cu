@@ -167,113 +167,70 @@ panel_rows_kernel(u64 *__restrict__ M, i64 ld, i64 wc, i64 w, const PanelState *
 }
 
 // ---------------------------------------------------------------- panel_update
-namespace {
-constexpr int UPD_TW = 4;      // words per CTA column tile
-constexpr int UPD_RT = 1024;   // rows per CTA row tile
-}  // namespace
+// Four-Russians update with tables of K pivot bits (M4RI k = K).  The panel's
+// 64 bit positions are cut into G = ceil(64/K) groups of consecutive
+// positions (the last one shorter when K does not divide 64); group g's table
+// holds the 2^bits(g) XOR combinations of the reduced rows R of its positions
+// (zero rows where a position holds no pivot), built level by level: entry v
+// = entry (v - 2^h) ^ entry 2^h for v in (2^h, 2^(h+1)).  Every other row j
+// (active rows for the rank; all rows for the RREF) then XORs, per word,
+// one entry per group, indexed by its panel bits at the pivot positions.
+// Each CTA covers TW words (columns) and `rt` rows; the table build is paid
+// once per CTA, so a larger K (fewer lookups per row) pays off with more
+// rows per CTA.  Shared memory: (G-1)*2^K + 2^bits(G-1) entries of TW words.
+template <int K>
+struct M4riGroups {
+    static constexpr int G = (64 + K - 1) / K;
+    static constexpr int last_bits = 64 - (G - 1) * K;
+    static constexpr int entries = (G - 1) * (1 << K) + (1 << last_bits);
+    __host__ __device__ static constexpr int bits(int g) { return g == G - 1 ? last_bits : K; }
+};
 
+template <int K, int TW>
 __global__ void __launch_bounds__(256)
 panel_update_kernel(u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const PanelState *ps,
                     const u64 *__restrict__ Rbuf, const unsigned char *state, const int *stamp,
-                    int panel, int rref, const u64 *__restrict__ ysnap)
+                    int panel, int rref, const u64 *__restrict__ ysnap, int rt)
 {
+    using Gr = M4riGroups<K>;
     extern __shared__ __align__(16) unsigned char upd_raw[];
-    auto T = reinterpret_cast<u64 (*)[256][UPD_TW]>(upd_raw);  // [8][256][UPD_TW]
+    u64 *T = reinterpret_cast<u64 *>(upd_raw);  // entry e of group g: T[((g << K) + e) * TW + t]
     const int p = ps->p;
     if (p == 0) return;
     const u64 pm = ps->pivmask;
-    const i64 w0 = w + (i64)blockIdx.x * UPD_TW;
+    const i64 w0 = w + (i64)blockIdx.x * TW;
     const int tid = threadIdx.x;
 
-    // level 0: T[g][0] = 0 and T[g][1<<h] = R'(8g+h) for every bit h
-    for (int e = tid; e < 8 * 9 * UPD_TW; e += 256) {
-        const int t = e % UPD_TW, gh = e / UPD_TW, g = gh / 9, h = gh % 9;
+    // level 0: entry 0 of every group is zero, entry 2^h of group g is R'(gK + h)
+    for (int e = tid; e < Gr::G * TW; e += 256) T[(((e / TW) << K)) * TW + e % TW] = 0;
+    for (int e = tid; e < 64 * TW; e += 256) {
+        const int t = e % TW, b = e / TW, g = b / K, h = b - g * K;
         const i64 word = w0 + t;
-        if (h == 8) {
-            T[g][0][t] = 0;
-            continue;
-        }
-        const int b = 8 * g + h;
         u64 v = 0;
         if (((pm >> b) & 1) && word < wc) {
             const int k = __popcll(pm & ((1ull << b) - 1));
             v = Rbuf[(i64)k * wc + word];
         }
-        T[g][1 << h][t] = v;
+        T[((g << K) + (1 << h)) * TW + t] = v;
     }
     __syncthreads();
-    // levels h = 1..7: T[v] = T[v - 2^h] ^ T[2^h] for v in (2^h, 2^(h+1))
-    for (int h = 1; h < 8; ++h) {
+#pragma unroll 1
+    for (int h = 1; h < K; ++h) {
         const int cnt = (1 << h) - 1;
-        for (int e = tid; e < 8 * cnt * UPD_TW; e += 256) {
-            const int t = e % UPD_TW, rest = e / UPD_TW, g = rest / cnt, v = (1 << h) + 1 + rest % cnt;
-            T[g][v][t] = T[g][v - (1 << h)][t] ^ T[g][1 << h][t];
+        for (int e = tid; e < Gr::G * cnt * TW; e += 256) {
+            const int t = e % TW, rest = e / TW, g = rest / cnt, v = (1 << h) + 1 + rest % cnt;
+            if (h < Gr::bits(g)) {
+                u64 *Tg = T + ((size_t)g << K) * TW;
+                Tg[v * TW + t] = Tg[(v - (1 << h)) * TW + t] ^ Tg[(1 << h) * TW + t];
+            }
         }
         __syncthreads();
     }
 
-    const i64 row0 = (i64)blockIdx.y * UPD_RT;
-    const int t = tid % UPD_TW;
+    const i64 row0 = (i64)blockIdx.y * rt;
+    const int t = tid % TW;
     const i64 word = w0 + t;
-    for (int rr = tid / UPD_TW; rr < UPD_RT; rr += 256 / UPD_TW) {
-        const i64 j = row0 + rr;
-        if (j >= m) break;
-        if (rref ? (stamp[j] == panel) : (state[j] == 0)) continue;
-        const u64 y = ysnap[j] & pm;
-        if (!y) continue;
-        if (word >= wc) continue;
-        u64 acc = 0;
-#pragma unroll
-        for (int g = 0; g < 8; ++g) acc ^= T[g][(y >> (8 * g)) & 255][t];
-        M[j * ld + word] ^= acc;
-    }
-}
-
-// 4-bit variant: 16 tables of the 16 combinations of 4 R rows (k = 4); a row
-// looks up 16 entries per word instead of 8, but a table costs 16x less to
-// build -- the better choice when few rows share a panel.
-namespace {
-constexpr int UPD4_TW = 8;
-}
-__global__ void __launch_bounds__(256)
-panel_update_k4_kernel(u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const PanelState *ps,
-                       const u64 *__restrict__ Rbuf, const unsigned char *state, const int *stamp,
-                       int panel, int rref, const u64 *__restrict__ ysnap)
-{
-    __shared__ u64 T[16][16][UPD4_TW];
-    const int p = ps->p;
-    if (p == 0) return;
-    const u64 pm = ps->pivmask;
-    const i64 w0 = w + (i64)blockIdx.x * UPD4_TW;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < 16 * 5 * UPD4_TW; e += 256) {
-        const int t = e % UPD4_TW, gh = e / UPD4_TW, g = gh / 5, h = gh % 5;
-        const i64 word = w0 + t;
-        if (h == 4) {
-            T[g][0][t] = 0;
-            continue;
-        }
-        const int b = 4 * g + h;
-        u64 v = 0;
-        if (((pm >> b) & 1) && word < wc) {
-            const int k = __popcll(pm & ((1ull << b) - 1));
-            v = Rbuf[(i64)k * wc + word];
-        }
-        T[g][1 << h][t] = v;
-    }
-    __syncthreads();
-    for (int h = 1; h < 4; ++h) {
-        const int cnt = (1 << h) - 1;
-        for (int e = tid; e < 16 * cnt * UPD4_TW; e += 256) {
-            const int t = e % UPD4_TW, rest = e / UPD4_TW, g = rest / cnt, v = (1 << h) + 1 + rest % cnt;
-            T[g][v][t] = T[g][v - (1 << h)][t] ^ T[g][1 << h][t];
-        }
-        __syncthreads();
-    }
-    const i64 row0 = (i64)blockIdx.y * UPD_RT;
-    const int t = tid % UPD4_TW;
-    const i64 word = w0 + t;
-    for (int rr = tid / UPD4_TW; rr < UPD_RT; rr += 256 / UPD4_TW) {
+    for (int rr = tid / TW; rr < rt; rr += 256 / TW) {
         const i64 j = row0 + rr;
         if (j >= m) break;
         if (rref ? (stamp[j] == panel) : (state[j] == 0)) continue;
@@ -281,8 +238,57 @@ panel_update_k4_kernel(u64 *__restrict__ M, i64 ld, i64 m, i64 wc, i64 w, const 
         if (!y || word >= wc) continue;
         u64 acc = 0;
 #pragma unroll
-        for (int g = 0; g < 16; ++g) acc ^= T[g][(y >> (4 * g)) & 15][t];
+        for (int g = 0; g < Gr::G; ++g)
+            acc ^= T[((g << K) + (int)((y >> (g * K)) & ((1ull << Gr::bits(g)) - 1))) * TW + t];
         M[j * ld + word] ^= acc;
+    }
+}
+
+// The (K, TW) pairs the blocked form runs with: TW (words per CTA) shrinks as
+// the tables grow, keeping them within 100 KB of shared memory.
+template <int K>
+struct M4riTile;
+template <> struct M4riTile<4> { static constexpr int TW = 8; };
+template <> struct M4riTile<6> { static constexpr int TW = 8; };
+template <> struct M4riTile<7> { static constexpr int TW = 4; };
+template <> struct M4riTile<8> { static constexpr int TW = 4; };
+template <> struct M4riTile<9> { static constexpr int TW = 2; };
+template <> struct M4riTile<10> { static constexpr int TW = 2; };
+
+template <int K>
+static mela_status launch_panel_update(u64 *M, i64 ld, i64 m, i64 wc, i64 w, const PanelState *ps,
+                                       const u64 *Rbuf, const unsigned char *state, const int *stamp,
+                                       int panel, int rref, const u64 *ysnap, int rt, cudaStream_t s,
+                                       bool configure)
+{
+    constexpr int TW = M4riTile<K>::TW;
+    constexpr size_t smem = (size_t)M4riGroups<K>::entries * TW * 8;
+    if (configure) {
+        MELA_CUDA_TRY(cudaFuncSetAttribute(panel_update_kernel<K, TW>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        return MELA_OK;
+    }
+    const i64 rem = wc - w;
+    const i64 rtiles = (m + rt - 1) / rt;
+    panel_update_kernel<K, TW><<<dim3((unsigned)((rem + TW - 1) / TW), (unsigned)rtiles), 256, smem, s>>>(
+        M, ld, m, wc, w, ps, Rbuf, state, stamp, panel, rref, ysnap, rt);
+    return MELA_OK;
+}
+
+using PanelUpdateFn = mela_status (*)(u64 *, i64, i64, i64, i64, const PanelState *, const u64 *,
+                                      const unsigned char *, const int *, int, int, const u64 *, int,
+                                      cudaStream_t, bool);
+
+static PanelUpdateFn panel_update_for(int k)
+{
+    switch (k) {
+    case 4: return launch_panel_update<4>;
+    case 6: return launch_panel_update<6>;
+    case 7: return launch_panel_update<7>;
+    case 8: return launch_panel_update<8>;
+    case 9: return launch_panel_update<9>;
+    case 10: return launch_panel_update<10>;
+    default: return nullptr;
     }
 }
 
@@ -544,20 +550,17 @@ size_t elim_workspace(i64 m, i64 n)
     return ab > c ? ab : c;
 }
 
-int choose_elim_variant(i64 m, i64 n, int rref)
-{
-    const int c = costmodel_choose(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0, 0.5);
-    static const int order[5] = {MELA_ELIM_PLAIN, MELA_ELIM_M4RI, MELA_ELIM_M4RI_K4, MELA_ELIM_FUSED, MELA_ELIM_TC};
-    if (c >= 0 && c < 5) return order[c];
-    // fixed rule: one CTA for small matrices, tensor-core windows otherwise
-    return (double)m * (double)n < 8192.0 ? MELA_ELIM_FUSED : MELA_ELIM_TC;
-}
-
-mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank,
+mela_status elim_device(int variant_arg, u64 *M, i64 ld, i64 m, i64 n, int rref, long long *d_rank,
                         long long *d_piv, long long *d_prow, void *ws, size_t ws_bytes,
                         cudaStream_t s)
 {
-    if (variant == MELA_ELIM_AUTO) variant = choose_elim_variant(m, n, rref);
+    Tuning tune{};
+    if (m > 0 && n > 0) variant_arg = resolve_elim_variant(variant_arg, M, ld, m, n, rref, s);
+    if (!decode_elim_variant(variant_arg, &tune)) {
+        set_error("elimination: bad variant argument 0x%x", variant_arg);
+        return MELA_ERR_INVALID;
+    }
+    const int variant = tune.base;
     if (m == 0 || n == 0) {
         MELA_CUDA_TRY(cudaMemsetAsync(d_rank, 0, sizeof(long long), s));
         return MELA_OK;
@@ -624,26 +627,23 @@ mela_status elim_device(int variant, u64 *M, i64 ld, i64 m, i64 n, int rref, lon
     const size_t sel_smem = sizeof(SelSmem);
     MELA_CUDA_TRY(cudaFuncSetAttribute(panel_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sel_smem));
-    const i64 rtiles = (m + UPD_RT - 1) / UPD_RT;
-    if (rtiles > 65535) {
-        set_error("elimination: too many rows for one update launch");
-        return MELA_ERR_UNSUPPORTED;
+    const PanelUpdateFn update = panel_update_for(tune.k);
+    if (!update) {
+        set_error("blocked elimination: M4RI k = %d (4 or 6..10 supported)", tune.k);
+        return MELA_ERR_INVALID;
     }
-    const size_t upd_smem = (size_t)8 * 256 * UPD_TW * 8;
-    MELA_CUDA_TRY(cudaFuncSetAttribute(panel_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)upd_smem));
+    const int rt = tune.row_tile;
+    if (mela_status st = check_grid_yz((m + rt - 1) / rt, 1, "blocked elimination update"); st != MELA_OK)
+        return st;
+    if (mela_status st = update(M, ld, m, wc, 0, ps, rbuf, state, stamp, 0, rref, ysnap, rt, s, true);
+        st != MELA_OK)
+        return st;
     for (i64 pw = 0; pw < wc; ++pw) {  // every word column is one panel
         panel_select_kernel<<<1, 1024, sel_smem, s>>>(M, ld, m, pw, state, stamp, (int)pw, ps,
                                                        d_piv, d_prow, ysnap);
         const i64 rem = wc - pw;
         panel_rows_kernel<<<(unsigned)((rem + 31) / 32), 256, 0, s>>>(M, ld, wc, pw, ps, rbuf);
-        if (variant == MELA_ELIM_M4RI_K4)
-            panel_update_k4_kernel<<<dim3((unsigned)((rem + UPD4_TW - 1) / UPD4_TW), (unsigned)rtiles), 256, 0,
-                                     s>>>(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref, ysnap);
-        else
-            panel_update_kernel<<<dim3((unsigned)((rem + UPD_TW - 1) / UPD_TW), (unsigned)rtiles), 256,
-                                  upd_smem, s>>>(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref,
-                                                 ysnap);
+        update(M, ld, m, wc, pw, ps, rbuf, state, stamp, (int)pw, rref, ysnap, rt, s, false);
     }
     MELA_LAUNCH_CHECK("panel elimination");
     MELA_CUDA_TRY(cudaMemcpyAsync(d_rank, &ps->rank, sizeof(long long), cudaMemcpyDeviceToDevice, s));

@@ -15,7 +15,6 @@ struct NullLayout {
 
 ElimLayout elim_layout(i64 m, i64 n);
 size_t elim_workspace(i64 m, i64 n);
-int choose_elim_variant(i64 m, i64 n, int rref);
 
 // Rank (rref = 0) or reduced row echelon form (rref = 1) of the packed m x n
 // matrix M, in place.  Writes the rank to d_rank, the pivot columns to d_piv

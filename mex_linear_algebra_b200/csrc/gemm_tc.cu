@@ -479,16 +479,18 @@ mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 
 }
 
 // CTA pairs are used whenever the padded row count allows (mp % 256 == 0),
-// unless MELA_TC_PAIR=0 is set in the environment (one CTA per 128 x 256 tile).
-static bool use_pairs(i64 mp)
+// unless the tile choice asks for single CTAs (tile 1) or, for the default
+// choice, MELA_TC_PAIR=0 is set in the environment.
+static bool use_pairs(i64 mp, int tile)
 {
-    if (mp % 256) return false;
+    if (mp % 256 || tile == 1) return false;
+    if (tile == 2) return true;
     const char *e = getenv("MELA_TC_PAIR");
     return !(e && e[0] == '0');
 }
 
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
-                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4)
+                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4, int tile)
 {
     if (m <= 0 || n <= 0) return MELA_OK;
     if (mp % BM || np % BN || kp % BK || kp <= 0) {
@@ -504,7 +506,7 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
         set_error("gemm_tc: problem too large for one launch");
         return MELA_ERR_UNSUPPORTED;
     }
-    if (use_pairs(mp)) {
+    if (use_pairs(mp, tile)) {
         CUtensorMap ma, mb;
         mela_status st = make_map(&ma, A8, mp, kp, 128);
         if (st != MELA_OK) return st;

@@ -186,7 +186,8 @@ extern "C" size_t mela_elim_workspace_size(int64_t m, int64_t n)
 
 static mela_status check_elim(int32_t variant, const uint64_t *dM, int64_t ld, int64_t m, int64_t n)
 {
-    if (m < 0 || n < 0 || ld < words_of(n) || variant < MELA_ELIM_AUTO || variant > MELA_ELIM_TC) {
+    Tuning t;
+    if (m < 0 || n < 0 || ld < words_of(n) || !decode_elim_variant(variant, &t)) {
         set_error("bad shape, leading dimension or variant");
         return MELA_ERR_INVALID;
     }

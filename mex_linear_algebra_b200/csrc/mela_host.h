@@ -33,10 +33,44 @@ mela_status finish(cudaStream_t s);
 // Row pitch in words, rounded up to an even count (16-byte rows).
 i64 even_words(i64 bits);
 
-int choose_gemm_variant(i64 m, i64 k, i64 n);
-// Learned cost model: variant index 0..2 for the request, or -1 without a model.
-int costmodel_choose(int op, double m, double n, double p, double density);
-void costmodel_features(int op, double m, double n, double p, double density, float *x);
+// A variant argument split into its base variant and tuning fields
+// (MELA_TUNE_K / MELA_TUNE_TILE of include/mela.h), defaults filled in.
+struct Tuning {
+    int base;      // mela_gemm_variant or mela_elim_variant
+    int k;         // Four-Russians table width (M4RI forms)
+    int row_tile;  // rows per update CTA (blocked elimination)
+    int tc_tile;   // tensor-core products: 0 default, 1 single CTAs, 2 CTA pairs
+};
+// false when a field is out of range for the base variant
+bool decode_elim_variant(int32_t v, Tuning *t);
+bool decode_gemm_variant(int32_t v, Tuning *t);
+
+// Configurations of an op in the cost model's output order (dispatch.cu).
+int config_count(int op);
+int32_t config_variant(int op, int index);
+// AUTO -> a concrete variant argument: the installed model's choice for the
+// input's measured density, else the fixed rule.  Other variants pass through.
+int32_t resolve_gemm_variant(int32_t variant, const u64 *A, i64 lda, i64 m, i64 k, i64 n, cudaStream_t s);
+int32_t resolve_elim_variant(int32_t variant, const u64 *M, i64 ld, i64 m, i64 n, int rref, cudaStream_t s);
+int32_t fixed_gemm_variant(i64 m, i64 k, i64 n);
+int32_t fixed_elim_variant(i64 m, i64 n);
+// Ones of a packed matrix, stream-ordered, into d_count (device).
+mela_status launch_popcount(const u64 *M, i64 ld, i64 m, i64 n, long long *d_count, cudaStream_t s);
+// Density of a packed device matrix, read back (waits for s); 0.5 while s is
+// being captured or on failure.
+double measure_density(const u64 *M, i64 ld, i64 m, i64 n, cudaStream_t s);
+
+// Learned cost model (mlp.cu): configuration index for the request, or -1
+// without a model.
+bool costmodel_loaded();
+int costmodel_choose(int op, double m, double n, double p, double density, double batch_count,
+                     double batch_log2_cells);
+// Predicted log2 microseconds of every configuration of the request
+// (config_count(op) values); false without a model.
+bool costmodel_predict(int op, double m, double n, double p, double density, double batch_count,
+                       double batch_log2_cells, float *y);
+void costmodel_features(int op, double m, double n, double p, double density, double batch_count,
+                        double batch_log2_cells, float *x);
 size_t gemm_workspace(int variant, i64 m, i64 k, i64 n);
 mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, i64 m, i64 k,
                          i64 n, void *ws, size_t ws_bytes, cudaStream_t s);

@@ -36,8 +36,10 @@ mela_status launch_gemm_plain(const u64 *A, i64 lda, const u64 *Bt, i64 ldbt, u6
 // both K-major; mp % 128 == 0, np % 256 == 0, kp % 128 == 0.  Writes the
 // valid m x n block of packed C.
 // fp4 = true: packed e2m1 operands (kp counts bytes, two values each), kind::mxf4.
+// tile: 0 = CTA pairs (256 x 256 tiles) when mp % 256 == 0, else one CTA per
+// 128 x 256 tile; 1 = always one CTA per tile; 2 = pairs where mp allows.
 mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i64 mp, i64 np,
-                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4);
+                           i64 kp, u64 *C, i64 ldc, i64 m, i64 n, cudaStream_t s, bool fp4, int tile = 0);
 // TMA map of a K-major byte matrix rows x kp (row pitch kp bytes): boxes of
 // 128 bytes x box_rows rows with 128-byte swizzle, as the tcgen05 kernels read them.
 mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 rows, i64 kp, int box_rows);

@@ -2,11 +2,13 @@
 // hand-written kernels, used to choose how (never what) each request is
 // computed.
 //
-// Network: x (8 features) -> 32 ReLU -> 32 ReLU -> 5 outputs, the predicted
-// log2 running time (microseconds) of each of the request's kernel variants
-// (four products, five eliminations).  Parameters are one flat float array:
-//   W1[8][32] b1[32] W2[32][32] b2[32] W3[32][5] b3[5]   (1509 floats)
-// Loss: mean squared error over the observed (sample, variant) pairs.
+// Network: x (MELA_MLP_IN features) -> 32 ReLU -> 32 ReLU -> MELA_MLP_OUT
+// outputs, the predicted log2 running time (microseconds) of each
+// configuration of the request's op (dispatch.cu lists them: ten
+// elimination configurations, six product configurations, three batch
+// engines).  Parameters are one flat float array:
+//   W1[IN][H1] b1[H1] W2[H1][H2] b2[H2] W3[H2][OUT] b3[OUT]
+// Loss: mean squared error over the observed (sample, configuration) pairs.
 //
 // Kernels: forward (one thread per sample), backward (one thread per sample,
 // per-block gradient sums in shared memory, then one global atomic per
@@ -155,9 +157,21 @@ __global__ void adam_kernel(float *__restrict__ params, const float *__restrict_
 // ---------------------------------------------------------------- host-side model
 // The dispatch copy of the trained parameters (host memory): single calls
 // evaluate the tiny network on the host to pick a variant before launching.
+// The model trained with the library (costmodel.json, compiled in by the
+// build) is installed when the library loads; mela_costmodel_load replaces
+// or removes it.
+#include "costmodel_weights.inc"
 static std::mutex g_cm_mu;
 static float g_cm[kParams];
 static bool g_cm_loaded = false;
+#ifdef MELA_DEFAULT_MODEL
+static_assert(sizeof kDefaultModel / sizeof kDefaultModel[0] == kParams, "compiled-in model size");
+static const bool g_cm_default = [] {
+    std::memcpy(g_cm, kDefaultModel, sizeof g_cm);
+    g_cm_loaded = true;
+    return true;
+}();
+#endif
 
 static void host_forward(const float *P, const float *x, float *y)
 {
@@ -179,7 +193,8 @@ static void host_forward(const float *P, const float *x, float *y)
     }
 }
 
-void costmodel_features(int op, double m, double n, double p, double density, float *x)
+void costmodel_features(int op, double m, double n, double p, double density, double batch_count,
+                        double batch_log2_cells, float *x)
 {
     auto lg = [](double v) { return (float)(std::log2(v > 1 ? v : 1) / 14.0); };
     x[0] = lg(m);
@@ -190,25 +205,44 @@ void costmodel_features(int op, double m, double n, double p, double density, fl
     x[4] = op == MELA_OP_RANK ? 1.f : 0.f;
     x[5] = op == MELA_OP_NULL ? 1.f : 0.f;
     x[6] = op == MELA_OP_MATMUL ? 1.f : 0.f;
-    x[7] = 1.f;
+    x[7] = op == MELA_OP_BATCH ? 1.f : 0.f;
+    // batch mix: how many matrices share the launch, and how large they are
+    x[8] = (float)(std::log2(batch_count > 1 ? batch_count : 1) / 16.0);
+    x[9] = (float)(batch_log2_cells / 28.0);
 }
 
-// -1 when no model is loaded (callers use their fixed rule)
-int costmodel_choose(int op, double m, double n, double p, double density)
+bool costmodel_loaded()
+{
+    std::lock_guard<std::mutex> g(g_cm_mu);
+    return g_cm_loaded;
+}
+
+bool costmodel_predict(int op, double m, double n, double p, double density, double batch_count,
+                       double batch_log2_cells, float *y_out)
 {
     float P[kParams];
     {
         std::lock_guard<std::mutex> g(g_cm_mu);
-        if (!g_cm_loaded) return -1;
+        if (!g_cm_loaded) return false;
         std::memcpy(P, g_cm, sizeof P);
     }
     float x[kIn], y[kOut];
-    costmodel_features(op, m, n, p, density, x);
+    costmodel_features(op, m, n, p, density, batch_count, batch_log2_cells, x);
     host_forward(P, x, y);
-    // products: plain, m4ri, tc, tc_fp4; elimination: plain, m4ri, m4ri_k4, fused, tc
-    const int nv = op == MELA_OP_MATMUL ? 4 : 5;
+    const int nc = config_count(op);
+    for (int o = 0; o < nc; ++o) y_out[o] = y[o];
+    return true;
+}
+
+// -1 when no model is loaded (callers use their fixed rule)
+int costmodel_choose(int op, double m, double n, double p, double density, double batch_count,
+                     double batch_log2_cells)
+{
+    float y[kOut];
+    const int nc = config_count(op);
+    if (nc <= 0 || !costmodel_predict(op, m, n, p, density, batch_count, batch_log2_cells, y)) return -1;
     int best = 0;
-    for (int o = 1; o < nv; ++o)
+    for (int o = 1; o < nc; ++o)
         if (y[o] < y[best]) best = o;
     return best;
 }
@@ -275,13 +309,15 @@ extern "C" mela_status mela_costmodel_load(const float *h_params)
     return MELA_OK;
 }
 
-extern "C" int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density)
+extern "C" int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density,
+                                         int64_t batch_count, double batch_log2_cells)
 {
-    return costmodel_choose(op, (double)m, (double)n, (double)p, density);
+    return costmodel_choose(op, (double)m, (double)n, (double)p, density, (double)batch_count,
+                            batch_log2_cells);
 }
 
 extern "C" void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
-                                        float *x)
+                                        int64_t batch_count, double batch_log2_cells, float *x)
 {
-    costmodel_features(op, (double)m, (double)n, (double)p, density, x);
+    costmodel_features(op, (double)m, (double)n, (double)p, density, (double)batch_count, batch_log2_cells, x);
 }

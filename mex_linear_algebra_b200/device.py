@@ -115,7 +115,10 @@ class BatchPlan:
     (``z_offsets``).
     """
 
-    def __init__(self, shapes, force_class: int = -1):
+    def __init__(self, shapes, force_class: int = -1, densities=None):
+        """force_class: the engine policy -- -1 the size rule, 0/1/2 that
+        engine wherever it fits, -2 the installed cost model's choice per
+        matrix (from its shape, ``densities`` and the batch mix)."""
         import ctypes as C
         import numpy as np
         self.shapes = np.asarray(shapes, dtype=np.int64).reshape(-1, 2)
@@ -134,8 +137,26 @@ class BatchPlan:
         for i in range(cnt):
             items[i] = _lib.BatchItem(int(m[i]), int(n[i]), int(self.in_offsets[i]), int(self.z_offsets[i]))
         self._plan = C.c_void_p()
-        check(lib().mela_batch_plan_create(items, cnt, force_class, C.byref(self._plan)))
+        self._items = items
+        if densities is None:
+            check(lib().mela_batch_plan_create_ex(items, cnt, None, force_class, C.byref(self._plan)))
+        else:
+            dens = np.ascontiguousarray(densities, dtype=np.float64)
+            if dens.shape != (cnt,):
+                raise ValueError("one density per matrix")
+            check(lib().mela_batch_plan_create_ex(items, cnt, dens.ctypes.data, force_class,
+                                                  C.byref(self._plan)))
         self.count = cnt
+
+    def densities(self, d_packed, stream=None):
+        """Fraction of ones of every matrix of a packed batch (in_offsets
+        layout), counted on the device."""
+        import numpy as np
+        cnt = torch.zeros(max(self.count, 1), dtype=torch.int64, device=d_packed.device)
+        check(lib().mela_batch_popcounts(self._items, self.count, _ptr(d_packed), _ptr(cnt), _stream(stream)))
+        ones = cnt[:self.count].cpu().numpy().astype(np.float64)
+        cells = (self.shapes[:, 0] * self.shapes[:, 1]).astype(np.float64)
+        return np.where(cells > 0, ones / np.maximum(cells, 1), 0.0)
 
     def stats(self):
         import ctypes as C

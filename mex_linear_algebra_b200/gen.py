@@ -19,6 +19,9 @@ Configurations (seeds as in the benchmark definitions):
   words 3.. of the same stream.
 * mixed request stream -- ``mixed_stream``: m, n, p log-uniform in
   [32, 8192], density log-uniform in [0.001, 0.5], aspect ratio <= 8:1.
+* batch requests -- ``batch_requests``: homogeneous batches for timing the
+  batched engines: m log-uniform in [32, 1024], n = m * [1, 3], density
+  log-uniform in [0.002, 0.5], 64 to 4096 matrices.
 """
 from __future__ import annotations
 
@@ -155,6 +158,28 @@ def mixed_stream(count: int = 50000, seed: int = 4):
     names = np.array(["rank", "null", "matmul"])[op]
     return [dict(op=str(names[i]), m=int(round(m[i])), n=int(round(n[i])), p=int(round(p[i])),
                  density=float(dens[i]), stream=i) for i in range(count)]
+
+
+def batch_requests(count: int, seed: int = 4, offset: int = 0):
+    """Batch requests: dicts with op 'batch', m, n, density and batch_count
+    (the number of m x n matrices in the batch).  Word layout per request r:
+    4 words of stream 1 at 4(offset + r).  Batches hold at most 2^30 bits."""
+    if count <= 0:
+        return []
+    w = words(seed, 1, 4 * offset, 4 * count).reshape(count, 4).astype(np.float64) / 2.0 ** 64
+    m = np.exp(np.log(32.0) + (np.log(1024.0) - np.log(32.0)) * w[:, 0])
+    n = m * (1.0 + 2.0 * w[:, 1])
+    dens = np.exp(np.log(0.002) + (np.log(0.5) - np.log(0.002)) * w[:, 2])
+    cnt = (64 * 4 ** np.floor(w[:, 3] * 4)).astype(np.int64)  # 64, 256, 1024, 4096
+    out = []
+    for i in range(count):
+        mi, ni = int(round(m[i])), int(round(n[i]))
+        c = int(cnt[i])
+        while c > 64 and c * mi * ni > (1 << 30):
+            c //= 4
+        out.append(dict(op="batch", m=mi, n=ni, p=0, density=float(dens[i]), batch_count=c,
+                        stream=offset + i))
+    return out
 
 
 def sparse_packed(seed: int, stream: int, m: int, n: int, density: float) -> np.ndarray:

@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY -- CPU oracle of the cost-model MLP.
 
 Float64 numpy restatement of the network in mex_linear_algebra_b200/csrc/
-mlp.cu (8 -> 32 ReLU -> 32 ReLU -> 5, flat parameters W1 b1 W2 b2 W3 b3,
+mlp.cu (10 -> 32 ReLU -> 32 ReLU -> 10, flat parameters W1 b1 W2 b2 W3 b3,
 masked mean squared error), with analytic gradients.  The GPU kernels are
 checked against it, and it is checked against central finite differences.
 The reference library has no learned component; this oracle pins the
@@ -9,7 +9,7 @@ project's own kernels.
 """
 import numpy as np
 
-IN, H1, H2, OUT = 8, 32, 32, 5
+IN, H1, H2, OUT = 10, 32, 32, 10
 SHAPES = [("W1", (IN, H1)), ("b1", (H1,)), ("W2", (H1, H2)), ("b2", (H2,)), ("W3", (H2, OUT)),
           ("b3", (OUT,))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SHAPES)

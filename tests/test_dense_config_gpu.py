@@ -44,9 +44,12 @@ def test_dense_rank_and_null_full_size(cuda):
     dr = torch.zeros(1, dtype=torch.int64, device="cuda")
     dpv = torch.empty(m, dtype=torch.int64, device="cuda")
     dpr = torch.empty(m, dtype=torch.int64, device="cuda")
-    for form in ("m4ri", "m4ri_k4", "plain", "tc"):
+    forms = {f: _lib.ELIM_VARIANTS[f] for f in ("m4ri", "m4ri_k4", "plain", "tc")}
+    forms["m4ri_k10_rt4096"] = _lib.tune(_lib.ELIM_M4RI, 10, 3)  # the reference rank_m4ri's own k
+    forms["m4ri_k6"] = _lib.tune(_lib.ELIM_M4RI, 6)
+    for form, v in forms.items():
         Mx = A.clone()
-        _lib.check(L.mela_dev_rank(_lib.ELIM_VARIANTS[form], Mx.data_ptr(), wc, m, n, dr.data_ptr(),
+        _lib.check(L.mela_dev_rank(v, Mx.data_ptr(), wc, m, n, dr.data_ptr(),
                                    dpv.data_ptr(), dpr.data_ptr(), ws.data_ptr(), wsb, s))
         assert int(dr.item()) == golden["rank"], form
     # RREF by the tensor-core form equals the blocked form's (pivots and rows)

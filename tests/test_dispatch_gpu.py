@@ -1,0 +1,140 @@
+"""How a request is computed never changes what it computes.
+
+* the tensor-core products on single CTAs and on CTA pairs (the tile field);
+* the device popcount the dispatcher's density comes from;
+* AUTO dispatch through an installed cost model, forced by the model's
+  weights onto each configuration in turn, for products and eliminations;
+* batched plans whose engine per matrix the cost model picks (with the
+  densities counted on the device), against the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import to_dev, to_host, valid_words
+
+pytestmark = pytest.mark.gpu
+
+
+def _forcing_model(op_count, index):
+    """Weights whose prediction is lowest for configuration `index` whatever
+    the input: zero weights, output biases 10 except 0 at `index`."""
+    from mex_linear_algebra_b200 import _lib
+    p = np.zeros(_lib.MLP_PARAMS, dtype=np.float32)
+    b3 = p[-_lib.MLP_OUT:]
+    b3[:] = 10.0
+    b3[index] = 0.0
+    return p
+
+
+@pytest.mark.parametrize("tile", [1, 2])
+@pytest.mark.parametrize("base", ["tc", "tc_fp4"])
+def test_tensor_core_tiles(cuda, base, tile):
+    from mex_linear_algebra_b200 import _lib, device as D
+    for (m, k, n) in [(300, 700, 500), (512, 1000, 256), (2048, 4096, 1024)]:
+        A, B = O.rand_dense(91, m, m, k), O.rand_dense(91, k, k, n)
+        v = _lib.tune(_lib.GEMM_VARIANTS[base], 0, tile)
+        got = to_host(D.matmul(to_dev(A), to_dev(B), m, k, n, variant=v))
+        assert np.array_equal(valid_words(got, n), O.matmul(A, B, m, k, n)), (m, k, n)
+
+
+def test_popcount(cuda):
+    import torch
+    from mex_linear_algebra_b200 import _lib
+    L = _lib.lib()
+    for (m, n) in [(1, 1), (37, 65), (1000, 3000), (5, 64)]:
+        P = O.rand_dense(92, m, m, n)
+        d = to_dev(P)
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        _lib.check(L.mela_dev_popcount(d.data_ptr(), d.shape[1], m, n, cnt.data_ptr(),
+                                       torch.cuda.current_stream().cuda_stream))
+        want = int(np.unpackbits(P.view(np.uint8)).sum())
+        assert int(cnt.item()) == want
+
+
+def test_auto_through_every_product_configuration(cuda):
+    from mex_linear_algebra_b200 import costmodel, device as D
+    m, k, n = 1500, 1100, 1300
+    A, B = O.rand_dense(93, 0, m, k), O.rand_dense(93, 1, k, n)
+    want = O.matmul(A, B, m, k, n)
+    try:
+        for i, name in enumerate(costmodel.CONFIG_NAMES["matmul"]):
+            costmodel.install(_forcing_model(6, i))
+            assert costmodel.choose("matmul", m, k, n, 0.5) == name
+            got = to_host(D.matmul(to_dev(A), to_dev(B), m, k, n, variant="auto"))
+            assert np.array_equal(valid_words(got, n), want), name
+    finally:
+        costmodel.install(None)
+
+
+@pytest.mark.parametrize("op", ["rank", "null"])
+def test_auto_through_every_elimination_configuration(cuda, op):
+    import torch
+    from mex_linear_algebra_b200 import _lib, costmodel
+    from test_elim_gpu import dev_null
+    L = _lib.lib()
+    m, n = 700, 1500
+    Lr, Rr = O.rand_dense(94, 0, m, 300), O.rand_dense(94, 1, 300, n)
+    P = O.matmul(Lr, Rr, m, 300, n)  # rank 300
+    want_R, want_piv = O.rref(P, m, n)
+    want_Z = O.null_basis_packed(P, m, n)
+    s = torch.cuda.current_stream().cuda_stream
+    try:
+        for i, name in enumerate(costmodel.CONFIG_NAMES[op]):
+            costmodel.install(_forcing_model(10, i))
+            assert costmodel.choose(op, m, n, 0, 0.5) == name
+            M = to_dev(P)
+            rank = torch.zeros(1, dtype=torch.int64, device="cuda")
+            piv = torch.empty(m, dtype=torch.int64, device="cuda")
+            prow = torch.empty(m, dtype=torch.int64, device="cuda")
+            wsb = L.mela_elim_workspace_size(m, n)
+            ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+            fn = L.mela_dev_rref if op == "null" else L.mela_dev_rank
+            _lib.check(fn(_lib.ELIM_AUTO, M.data_ptr(), M.shape[1], m, n, rank.data_ptr(), piv.data_ptr(),
+                          prow.data_ptr(), ws.data_ptr(), wsb, s))
+            r = int(rank.item())
+            assert r == len(want_piv), name
+            pv = to_host(piv)[:r].astype(np.int64)
+            assert np.array_equal(pv, want_piv), name
+            if op == "null":
+                Zt = dev_null(M, m, n, r, pv, to_host(prow)[:r].astype(np.int64))
+                assert np.array_equal(valid_words(Zt, n), want_Z), name
+    finally:
+        costmodel.install(None)
+
+
+def test_learned_batch_engines(cuda):
+    """Each engine forced through the model, and the densities counted on
+    the device: bit-exact against the oracle, matrix by matrix."""
+    import torch
+    from mex_linear_algebra_b200 import costmodel, device as D, gen
+    mats = [gen.ldpc_packed(3, b) for b in range(30)]
+    mats += [(m, n, O.rand_dense(95, i, m, n)) for i, (m, n) in enumerate([(40, 90), (100, 230), (300, 700)])]
+    shapes = [(m, n) for (m, n, _) in mats]
+    plan0 = D.BatchPlan(shapes)
+    buf = np.zeros(max(plan0.in_words, 1), dtype=np.uint64)
+    for i, (m, n, P) in enumerate(mats):
+        o = int(plan0.in_offsets[i])
+        buf[o:o + P.size] = P.ravel()
+    d_in = torch.from_numpy(buf.view(np.int64)).cuda()
+    dens = plan0.densities(d_in)
+    want_dens = [np.unpackbits(P.view(np.uint8)).sum() / (m * n) for (m, n, P) in mats]
+    assert np.allclose(dens, want_dens, rtol=0, atol=1e-12)
+    plan0.close()
+    try:
+        for c in range(3):
+            costmodel.install(_forcing_model(3, c))
+            plan = D.BatchPlan(shapes, force_class=-2, densities=dens)
+            st = plan.stats()
+            ranks, zt = plan.run(d_in)
+            rk = to_host(ranks)
+            z = to_host(zt)
+            for i, (m, n, P) in enumerate(mats):
+                assert rk[i] == O.rank(P, m, n), (c, i)
+                assert np.array_equal(plan.basis(z, rk, i), O.null_basis_packed(P, m, n)), (c, i)
+            # the forced engine took every matrix that fits it
+            if c == 0:
+                assert st["cta"] == len(mats)
+            plan.close()
+    finally:
+        costmodel.install(None)

@@ -16,7 +16,18 @@ from gpu_util import to_dev, to_host, valid_words
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ("plain", "m4ri", "m4ri_k4", "fused", "tc")
+FORMS = ("plain", "m4ri", "m4ri_k4", "fused", "tc",
+         # the blocked form's tuning: Four-Russians k and rows per update CTA
+         "m4ri_k6", "m4ri_k7", "m4ri_k9_rt4096", "m4ri_k10_rt4096", "m4ri_k8_rt256", "m4ri_k10_rt256")
+
+
+def variant_of(form):
+    from mex_linear_algebra_b200 import _lib
+    if form in _lib.ELIM_VARIANTS:
+        return _lib.ELIM_VARIANTS[form]
+    k, _, rt = form[len("m4ri_k"):].partition("_rt")
+    tile = {"": 0, "256": 1, "1024": 2, "4096": 3}[rt]
+    return _lib.tune(_lib.ELIM_M4RI, int(k), tile)
 
 
 def dev_rref(P, m, n, form, rref=True):
@@ -32,7 +43,7 @@ def dev_rref(P, m, n, form, rref=True):
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
     fn = L.mela_dev_rref if rref else L.mela_dev_rank
     s = torch.cuda.current_stream().cuda_stream
-    _lib.check(fn(_lib.ELIM_VARIANTS[form], M.data_ptr(), M.shape[1], m, n, rank.data_ptr(),
+    _lib.check(fn(variant_of(form), M.data_ptr(), M.shape[1], m, n, rank.data_ptr(),
                   piv.data_ptr(), prow.data_ptr(), ws.data_ptr(), wsb, s))
     r = int(rank.item())
     return M, r, to_host(piv)[:r].astype(np.int64), to_host(prow)[:r].astype(np.int64)

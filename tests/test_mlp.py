@@ -36,9 +36,54 @@ def test_parameter_count_matches_library():
 def test_features_are_scaled_log_shapes():
     from mex_linear_algebra_b200 import costmodel
     x = costmodel.features("matmul", 1024, 2048, 4096, 0.01)
-    assert np.allclose(x, [10 / 14, 11 / 14, 12 / 14, -2 / 3 + 1, 0, 0, 1, 1], atol=1e-6)
+    assert np.allclose(x, [10 / 14, 11 / 14, 12 / 14, -2 / 3 + 1, 0, 0, 1, 0, 0, 21 / 28], atol=1e-6)
     x = costmodel.features("null", 32, 8192, 0, 0.5)
-    assert x[2] == 0 and x[5] == 1 and x[6] == 0
+    assert x[2] == 0 and x[5] == 1 and x[6] == 0 and x[7] == 0 and x[8] == 0
+    # batch mix: 4096 matrices of mean log2(m*n) 19.5
+    x = costmodel.features("batch", 700, 1500, 0, 0.004, 4096, 19.5)
+    assert x[7] == 1 and np.isclose(x[8], 12 / 16) and np.isclose(x[9], 19.5 / 28)
+
+
+def test_configurations_match_the_library():
+    """The Python names and the library's configuration table agree, and
+    every configuration is a valid variant argument."""
+    from mex_linear_algebra_b200 import _lib, costmodel
+    L = _lib.lib()
+    tune = _lib.tune
+    assert costmodel.config_codes("rank") == (
+        _lib.ELIM_PLAIN, _lib.ELIM_M4RI_K4, tune(_lib.ELIM_M4RI, 6), tune(_lib.ELIM_M4RI, 7),
+        tune(_lib.ELIM_M4RI, 8), tune(_lib.ELIM_M4RI, 8, 1), tune(_lib.ELIM_M4RI, 9, 3),
+        tune(_lib.ELIM_M4RI, 10, 3), _lib.ELIM_FUSED, _lib.ELIM_TC)
+    assert costmodel.config_codes("null") == costmodel.config_codes("rank")
+    assert costmodel.config_codes("matmul") == (
+        _lib.GEMM_PLAIN, _lib.GEMM_M4RI, tune(_lib.GEMM_TC, 0, 2), tune(_lib.GEMM_TC, 0, 1),
+        tune(_lib.GEMM_TC_FP4, 0, 2), tune(_lib.GEMM_TC_FP4, 0, 1))
+    assert costmodel.config_codes("batch") == (0, 1, 2)
+    for op in ("rank", "matmul", "batch"):
+        assert len(costmodel.CONFIG_NAMES[op]) == L.mela_costmodel_config_count(costmodel.OPS[op])
+        assert L.mela_costmodel_config(costmodel.OPS[op], len(costmodel.CONFIG_NAMES[op])) == -1
+    for v in costmodel.config_codes("matmul"):
+        assert L.mela_matmul_workspace_size(v, 2048, 2048, 2048) > 0 or v == _lib.GEMM_M4RI
+
+
+def test_bad_tuning_fields_are_rejected_before_device_work():
+    """Out-of-range tuning fields fail with MELA_ERR_INVALID up front (no
+    device is touched: fake pointers are never dereferenced)."""
+    import ctypes as C
+    from mex_linear_algebra_b200 import _lib
+    L = _lib.lib()
+    tune = _lib.tune
+    fake = C.c_void_p(64)
+    bad_elim = [tune(_lib.ELIM_M4RI, 5), tune(_lib.ELIM_M4RI, 11), tune(_lib.ELIM_M4RI_K4, 8),
+                tune(_lib.ELIM_M4RI, 8, 4), tune(_lib.ELIM_TC, 8), tune(_lib.ELIM_PLAIN, 0, 1), 1 << 16, 6]
+    for v in bad_elim:
+        for fn in (L.mela_dev_rank, L.mela_dev_rref):
+            assert fn(v, fake, 2, 100, 100, fake, fake, fake, fake, 1 << 20, None) == _lib.ERR_INVALID, hex(v)
+    bad_gemm = [tune(_lib.GEMM_TC, 0, 3), tune(_lib.GEMM_M4RI, 6), tune(_lib.GEMM_PLAIN, 0, 1), 5]
+    for v in bad_gemm:
+        assert L.mela_dev_matmul(v, fake, 2, fake, 2, fake, 2, 100, 100, 100, fake, 1 << 30, None) \
+            == _lib.ERR_INVALID, hex(v)
+        assert L.mela_matmul_workspace_size(v, 100, 100, 100) == 0
 
 
 @pytest.mark.gpu
@@ -81,7 +126,7 @@ def test_training_fits_a_timing_surface(cuda):
         m, n = (int(x) for x in np.exp(rng.uniform(np.log(32), np.log(8192), 2)))
         d = float(np.exp(rng.uniform(np.log(1e-3), np.log(0.5))))
         lg = np.log2(m) + np.log2(n)
-        t = {"plain": 2 ** (0.9 * lg - 3), "m4ri": 2 ** (0.6 * lg + 1), "m4ri_k4": 2 ** (0.7 * lg)}
+        t = {"plain": 2 ** (0.9 * lg - 3), "m4ri_k8": 2 ** (0.6 * lg + 1), "m4ri_k4": 2 ** (0.7 * lg)}
         recs.append({"op": "rank", "m": m, "n": n, "p": 0, "density": d, "times_us": t})
     params, loss = costmodel.train(recs[:400], steps=2500)
     rep = costmodel.evaluate(params, recs[400:])
@@ -92,35 +137,32 @@ def test_training_fits_a_timing_surface(cuda):
 @pytest.mark.skipif(not os.path.exists(os.path.join(DATA, "autotune_eval.json")),
                     reason="no timing database recorded yet")
 def test_trained_model_beats_fixed_rule():
-    """On held-out requests with every variant timed (recorded on B200 by the
-    autotuner), the installed model's choices cost less in total than the
-    fixed rule's, and its regret against the exhaustive best is smaller.
+    """On held-out requests with every configuration timed (recorded on B200
+    by the autotuner), the installed model's choices cost less in total than
+    the fixed rule's, and its regret against the exhaustive best is smaller.
     Host-side inference through the library's dispatcher; no GPU needed."""
     from mex_linear_algebra_b200 import costmodel
     params = costmodel.load()
     ev = json.load(open(os.path.join(DATA, "autotune_eval.json")))
+    assert all(r["agree"] for r in ev)  # every configuration returned the same bits
     costmodel.install(params)
     try:
         tot_model = tot_rule = tot_best = 0.0
+        per_model, per_rule = [], []
         for r in ev:
-            names = costmodel.VARIANT_NAMES[r["op"]]
             t = r["times_us"]
-            tot_best += min(t[x] for x in names)
-            tot_model += t[costmodel.choose(r["op"], r["m"], r["n"], r.get("p", 0), r["density"])]
-            tot_rule += t[costmodel.heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"])]
+            best = min(t.values())
+            tm = t[costmodel.choose(r["op"], r["m"], r["n"], r.get("p", 0), r["density"],
+                                    r.get("batch_count", 1), r.get("batch_log2_cells"))]
+            tr = t[costmodel.heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"], r.get("rule"))]
+            tot_best += best
+            tot_model += tm
+            tot_rule += tr
+            per_model.append(tm / best - 1)
+            per_rule.append(tr / best - 1)
     finally:
         costmodel.install(None)
-    assert all(r["agree"] for r in ev)  # every variant returned the same bits
     assert tot_model < tot_rule
     assert tot_model / tot_best - 1 < tot_rule / tot_best - 1
     # per request, too: the mean slowdown against the exhaustive best shrinks
-    rep = {}
-    costmodel.install(params)
-    try:
-        per_model = [r["times_us"][costmodel.choose(r["op"], r["m"], r["n"], r.get("p", 0), r["density"])]
-                     / min(r["times_us"].values()) - 1 for r in ev]
-    finally:
-        costmodel.install(None)
-    per_rule = [r["times_us"][costmodel.heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"])]
-                / min(r["times_us"].values()) - 1 for r in ev]
     assert np.mean(per_model) < np.mean(per_rule)
