@@ -283,6 +283,65 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
         z0 = int(plan.z_offsets[i])
         ok = ok and bool(torch.equal(Zt[:f].reshape(-1), zt[z0:z0 + f * wc]))
     base_rate = baseline_sample / t_base
+    # per matrix again, with the library's AUTO dispatch (the fused single-CTA
+    # or tensor-core forms, chosen per matrix) and buffers allocated once
+    mmax, nmax = int(shapes[:, 0].max()), int(shapes[:, 1].max())
+    wcmax = (nmax + 63) // 64
+    Mbuf = torch.empty(mmax * wcmax, dtype=torch.int64, device="cuda")
+    Zbuf = torch.empty(nmax * wcmax, dtype=torch.int64, device="cuda")
+    dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    dpv = torch.empty(mmax, dtype=torch.int64, device="cuda")
+    dpr = torch.empty(mmax, dtype=torch.int64, device="cuda")
+    wsb = max(L.mela_elim_workspace_size(int(a), int(b)) for a, b in shapes[idx])
+    wsp = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    nwb = max(L.mela_null_workspace_size(int(b), min(int(a), int(b))) for a, b in shapes[idx])
+    nws = torch.empty(nwb, dtype=torch.uint8, device="cuda")
+    ok_auto = True
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in idx:
+        m, n = int(shapes[i, 0]), int(shapes[i, 1])
+        wc = (n + 63) // 64
+        Mx = Mbuf[:m * wc].view(m, wc)
+        Mx.copy_(d_packed[offsets[i]:offsets[i] + m * wc].view(m, wc))
+        check(L.mela_dev_rref(_lib.ELIM_AUTO, Mx.data_ptr(), wc, m, n, dr.data_ptr(), dpv.data_ptr(),
+                              dpr.data_ptr(), wsp.data_ptr(), wsb, s))
+        r = int(dr.item())
+        check(L.mela_dev_null_basis(Mx.data_ptr(), wc, m, n, r, dpv.data_ptr(), dpr.data_ptr(),
+                                    Zbuf.data_ptr(), wc, nws.data_ptr(), nwb, s))
+        torch.cuda.synchronize()
+        ok_auto = ok_auto and r == int(rk_host[i])
+    t_auto = time.perf_counter() - t0
+    auto_rate = baseline_sample / t_auto
+    del Mbuf, Zbuf, wsp, nws
+    # the same batch with each matrix's engine picked by the cost model from
+    # its shape, its density (counted on the device) and the batch mix
+    learned = {}
+    try:
+        dens = plan.densities(d_packed)
+        lplan = D.BatchPlan(shapes, force_class=-2, densities=dens)
+        r2, z2 = lplan.outputs()
+        for _ in range(3):
+            lplan.run_logical(d_log, r2, z2)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            lplan.run_logical(d_log, r2, z2)
+        e1.record()
+        e1.synchronize()
+        lms = e0.elapsed_time(e1) / reps
+        same = bool(torch.equal(r2, ranks))
+        if same:  # the bases, matrix by matrix (words past each basis are not written)
+            zh, z2h = zt.cpu().numpy(), z2.cpu().numpy()
+            rkh = rk_host
+            same = all(np.array_equal(plan.basis(zh, rkh, i), lplan.basis(z2h, rkh, i)) for i in range(count))
+        learned = {"ms_per_batch": round(lms, 3), "speedup_vs_size_rule": round(ms / lms, 3),
+                   "classes": lplan.stats(), "results_match": same,
+                   "policy": "engine per matrix by the cost model (shape, device-counted density, batch mix)"}
+        lplan.close()
+        del r2, z2
+    except Exception as e:  # reported, not fatal
+        learned = {"error": f"{type(e).__name__}: {e}"}
     rate = count / (ms * 1e-3)
     in_bytes = plan.logical_bytes
     # forward-elimination work (rank m, pivots in the leading columns) and the bytes that must move
@@ -302,6 +361,12 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
                                            "pack-free packed input, plain RREF + null basis per matrix, "
                                            "host clock per matrix"},
             "speedup_vs_per_matrix": round(rate / base_rate, 1), "results_match": ok,
+            "per_matrix_auto": {"value": round(auto_rate, 1), "unit": "matrices/s", "ranks_match": ok_auto,
+                                "sample": f"the same {baseline_sample} matrices, mela_dev_rref with AUTO "
+                                          "(cost-model choice per matrix) + null basis, buffers allocated "
+                                          "once, host clock"},
+            "speedup_vs_per_matrix_auto": round(rate / auto_rate, 1),
+            "learned_engines": learned,
             "pack": {"ms": round(pack_ms, 3), "exact": pack_ok,
                      "gbs": round((in_bytes + plan.in_words * 8) / (pack_ms * 1e-3) / 1e9, 1),
                      "note": "batch_pack_kernel alone: logical bytes read + packed words written"},
@@ -312,6 +377,50 @@ def bench_batched(torch, count=20000, seed=3, baseline_sample=200):
                          "hbm_gbs": round((in_bytes + z_bytes) / (ms * 1e-3) / 1e9, 1),
                          "work_note": "sum over matrices of sum_p 2(m-p-1)(n-p): forward elimination "
                                       "with the pivots in the leading columns"}}
+
+
+def bench_batched_sharded(torch, ws, rank, count=20000, seed=3, reps=5):
+    """The parity-check batch split over the ranks by estimated cost
+    (parallel.shard_batch; no data exchange): each rank runs its share from
+    packed input in one persistent launch (graph replay), timed with CUDA
+    events, the maximum over ranks; ranks gathered on the host and checked
+    against the oracle's for all 20,000 matrices."""
+    import numpy as np
+    from mex_linear_algebra_b200 import device as D, gen, parallel
+    shapes, offsets, buf = gen.ldpc_batch(count, seed)
+    golden = np.load(os.path.join(ROOT, "tests", "golden", "ldpc_20000.npz"))["ranks"]
+    state = {}
+
+    def compute(idx):
+        sub = shapes[idx]
+        wcs = (sub[:, 1] + 63) // 64
+        packed = np.concatenate([buf[offsets[i]:offsets[i] + shapes[i, 0] * w] for i, w in zip(idx, wcs)])
+        plan = D.BatchPlan(sub)
+        d = torch.from_numpy(packed.view(np.int64)).cuda()
+        ranks, zt = plan.outputs()
+        for _ in range(3):
+            plan.run(d, ranks, zt)
+        torch.cuda.synchronize()
+        parallel.barrier(ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            plan.run(d, ranks, zt)
+        e1.record()
+        e1.synchronize()
+        state["ms"] = e0.elapsed_time(e1) / reps
+        state["mine"] = len(idx)
+        rk = ranks.cpu().numpy()
+        plan.close()
+        return {int(i): int(rk[j]) for j, i in enumerate(idx)}
+
+    merged, owners = parallel.run_sharded(shapes, ws, rank, compute)
+    ms = parallel.max_over_ranks(ws, state["ms"])
+    ok = all(merged[i] == int(golden[i]) for i in range(count))
+    return {"metric": "batched rank+null mats/s, sharded over ranks", "value": round(count / (ms * 1e-3), 1),
+            "unit": "matrices/s", "n_gpus": ws, "ms_per_batch_max_over_ranks": round(ms, 3),
+            "matrices_per_rank": [len(o) for o in owners], "ranks_match_oracle": ok,
+            "input": "packed, resident in HBM", "scaling": "strong (the 20,000 matrices split over the ranks)"}
 
 
 def bench_dense_rank(torch):
@@ -419,21 +528,122 @@ def bench_dense_rank(torch):
     return out
 
 
-def bench_dispatch(torch, count=200):
-    """Installed cost model vs fixed rule vs exhaustive best on a sample of
-    the mixed request stream (every variant timed live)."""
-    from mex_linear_algebra_b200 import autotune, costmodel
-    if not os.path.exists(costmodel.DEFAULT_MODEL):
-        return {"unavailable": "no trained cost model installed"}
-    params = costmodel.load()
-    # median of 3 after a warm-up: the tensor-core elimination captures its
-    # CUDA graph on the second call with the same buffers (the first timed one)
-    recs = autotune.build_db(count, 200000, reps=3, max_cells=2e7)
-    rep = costmodel.evaluate(params, recs)
-    rep["sample"] = f"{len(recs)} requests of the mixed stream (seed 4) from request 200000, " \
-                    "each variant timed (median of 3 after a warm-up)"
-    rep["all_variants_bit_identical"] = all(r["agree"] for r in recs)
-    return rep
+def bench_gateway_config(torch, reps=5):
+    """The drop-in call at its benchmark configuration: mela_matmul_gf2(A, B)
+    with A 2048 x 2048 and B 2048 x 1024 double 0/1 (seed 0), host arrays
+    in MATLAB layout, logical result -- through the library's gateway (the
+    code the MEX file runs) and through the reference's own gateway on the
+    host cores, on the same arrays; median of `reps` calls after two
+    warm-ups each."""
+    import hashlib
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from mex_linear_algebra_b200 import mela
+    m, k, n = 2048, 2048, 1024
+    A = O.unpack(O.rand_dense(0, 0, m, k), m, k).astype(np.float64)
+    B = O.unpack(O.rand_dense(0, 1, k, n), k, n).astype(np.float64)
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "config_digests.json")))["matmul_gateway_2048"]
+
+    def timed(fn):
+        for _ in range(2):
+            out = fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), out
+
+    t_gpu, C = timed(lambda: mela.mela_matmul_gf2(A, B))
+    ok = hashlib.blake2b(O.pack(C).tobytes(), digest_size=16).hexdigest() == golden["digest"]
+    line = {"config": "mela_matmul_gf2(A 2048x2048 double, B 2048x1024 double), seed 0, logical out",
+            "gpu_ms": round(t_gpu * 1e3, 3), "result_matches_reference_digest": ok,
+            "h2d_bytes": int(A.nbytes + B.nbytes), "d2h_bytes": int(m * n),
+            "timing": f"host clock around the call, median of {reps}"}
+    if O.ref_available():
+        os.environ.setdefault("OMP_DYNAMIC", "FALSE")
+        t_ref, Cr = timed(lambda: O.ref_call("mela_matmul_gf2", A, B)[0])
+        line.update({"reference_ms": round(t_ref * 1e3, 3), "reference_threads": O.num_threads(),
+                     "reference_isa": O.host_isa(), "speedup_vs_reference": round(t_ref / t_gpu, 2),
+                     "same_result_as_reference": bool(np.array_equal(Cr, C))})
+    return line
+
+
+def _stratified(reqs, per_bin, bins):
+    """`per_bin` requests from each of `bins` log-size bins of the request
+    list (bits touched: m*n, plus n*p for products), evenly spaced."""
+    import numpy as np
+    cells = np.array([r["m"] * r["n"] + (r["n"] * r["p"] if r["op"] == "matmul" else 0) for r in reqs],
+                     dtype=np.float64)
+    lg = np.log2(cells)
+    edges = np.linspace(lg.min(), lg.max() + 1e-9, bins + 1)
+    out = []
+    for b in range(bins):
+        idx = np.nonzero((lg >= edges[b]) & (lg < edges[b + 1]))[0]
+        if len(idx):
+            take = idx[np.linspace(0, len(idx) - 1, min(per_bin, len(idx))).astype(np.int64)]
+            out.extend(int(i) for i in np.unique(take))
+    return [reqs[i] for i in out]
+
+
+def bench_dispatch(torch, per_bin=14, bins=8):
+    """The learned dispatch on the mixed request stream (50,000 requests,
+    seed 4: rank, null space and products, m, n, p log-uniform in [32, 8192],
+    density log-uniform in [0.001, 0.5]): a sample stratified by request
+    size, every size up to 8192 x 8192 kept.  Per request: every
+    configuration timed (the exhaustive best), the library's own AUTO
+    dispatch (the compiled-in cost model; the input's density measured on
+    the device inside the call), and the fixed rule's configuration."""
+    import numpy as np
+    from mex_linear_algebra_b200 import _lib, autotune, costmodel, gen
+    from mex_linear_algebra_b200._lib import lib
+    if lib().mela_costmodel_choose(_lib.OP_RANK, 100, 100, 0, 0.5, 1, 13.3) < 0:
+        return {"unavailable": "the library was built without a trained cost model"}
+    sample = _stratified(gen.mixed_stream(50000, 4), per_bin, bins)
+    recs = []
+    t0 = time.time()
+    for r in sample:
+        recs.append(autotune.time_request(r, reps=2, extra={"auto": 0}))
+        torch.cuda.empty_cache()
+    tot = {"best": 0.0, "auto": 0.0, "rule": 0.0}
+    per = {"auto": [], "rule": []}
+    by_op = {}
+    for r in recs:
+        t = r["times_us"]
+        best = min(v for kname, v in t.items() if kname != "auto")
+        rule = t[costmodel.heuristic(r["op"], r["m"], r["n"], r.get("p", 0), r["density"])]
+        tot["best"] += best
+        tot["auto"] += t["auto"]
+        tot["rule"] += rule
+        per["auto"].append(t["auto"] / best - 1)
+        per["rule"].append(rule / best - 1)
+        o = by_op.setdefault(r["op"], {"requests": 0, "best_us": 0.0, "auto_us": 0.0, "rule_us": 0.0})
+        o["requests"] += 1
+        o["best_us"] += best
+        o["auto_us"] += t["auto"]
+        o["rule_us"] += rule
+    for o in by_op.values():
+        o["auto_regret"] = round(o["auto_us"] / o["best_us"] - 1, 4)
+        o["rule_regret"] = round(o["rule_us"] / o["best_us"] - 1, 4)
+        for kname in ("best_us", "auto_us", "rule_us"):
+            o[kname] = round(o[kname], 1)
+    return {"requests": len(recs),
+            "sample": f"{len(recs)} of the 50,000 requests (seed 4), {per_bin} per log2-size bin over {bins} "
+                      "bins from the smallest to the 8192 x 8192 ones; every configuration timed "
+                      "(median of 2 after a warm-up)",
+            "library_auto_regret": round(tot["auto"] / tot["best"] - 1, 4),
+            "fixed_rule_regret": round(tot["rule"] / tot["best"] - 1, 4),
+            "auto_speedup_vs_rule": round(tot["rule"] / tot["auto"], 4),
+            "mean_request_regret": {"auto": round(float(np.mean(per["auto"])), 4),
+                                    "rule": round(float(np.mean(per["rule"])), 4)},
+            "total_us": {k_: round(v, 1) for k_, v in tot.items()},
+            "by_op": by_op,
+            "all_configurations_bit_identical": all(r["agree"] for r in recs),
+            "seconds": round(time.time() - t0, 1),
+            "note": "auto = mela_dev_rank / mela_dev_rref (+ null basis) / mela_dev_matmul with the AUTO "
+                    "variant: one popcount of the input and an 8-byte read-back, the model on the host, "
+                    "then the chosen configuration"}
 
 
 def run_mela(args, ws, rank, local):
@@ -566,9 +776,16 @@ def run_mela(args, ws, rank, local):
     del hA, hB, hC
 
     extras = {}
+    if ws > 1 and not args.no_extras:
+        # every rank takes part (its share of the batch; the gather and the max are collectives)
+        try:
+            extras["batched_sharded"] = bench_batched_sharded(torch, ws, rank)
+        except Exception as e:  # reported, never silently dropped
+            extras["batched_sharded"] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
     if rank == 0 and not args.no_extras:
-        for name, fn in (("batched", bench_batched), ("dense_rank_null", bench_dense_rank),
-                         ("learned_dispatch", bench_dispatch)):
+        for name, fn in (("drop_in_gateway", bench_gateway_config), ("batched", bench_batched),
+                         ("dense_rank_null", bench_dense_rank), ("learned_dispatch", bench_dispatch)):
             try:
                 extras[name] = fn(torch)
             except Exception as e:  # reported, never silently dropped

@@ -411,6 +411,11 @@ mela_status mela_costmodel_load(const float *h_params);
  * pass batch_count = 1 and batch_log2_cells = log2(m * n). */
 int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                               int64_t batch_count, double batch_log2_cells);
+/* The installed model's predicted log2 microseconds of every configuration
+ * of the request into y (mela_costmodel_config_count(op) values); returns
+ * that count, or -1 when no model is installed. */
+int32_t mela_costmodel_predict(int32_t op, int64_t m, int64_t n, int64_t p, double density,
+                               int64_t batch_count, double batch_log2_cells, float *y);
 /* The MELA_MLP_IN input features of a request. */
 void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                              int64_t batch_count, double batch_log2_cells, float *x);

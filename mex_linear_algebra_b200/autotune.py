@@ -182,27 +182,45 @@ def time_request(req, reps=3, extra=None):
 
 
 def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 7e7, batch_count: int = 0,
-             verbose: bool = False):
+             verbose: bool = False, out: str | None = None, budget_s: float = 0.0):
     """Time `count` requests of the mixed stream from request `offset` on
     (requests above `max_cells` bits are skipped; the stream's largest,
-    8192 x 8192, is 6.7e7), then `batch_count` batch requests."""
+    8192 x 8192, is 6.7e7), then `batch_count` batch requests.  With `out`
+    the records so far are written there every 25 requests; with `budget_s`
+    each part stops once it has used its share of that many seconds."""
     import torch
     reqs = gen.mixed_stream(offset + count, SEED)[offset:]
     db = []
     t0 = time.time()
+
+    def save():
+        if out:
+            with open(out, "w") as f:
+                json.dump(db, f)
+    share = budget_s * (0.75 if batch_count else 1.0)
     for i, r in enumerate(reqs):
         cells = r["m"] * r["n"] + (r["n"] * r["p"] if r["op"] == "matmul" else 0)
         if cells > max_cells:
             continue
         db.append(time_request(r, reps))
-        if verbose and (i + 1) % 50 == 0:
-            print(f"{i + 1}/{count} timed, {time.time() - t0:.1f}s", flush=True)
         torch.cuda.empty_cache()
+        if (i + 1) % 25 == 0:
+            save()
+            if verbose:
+                print(f"{i + 1}/{count} timed, {time.time() - t0:.1f}s", flush=True)
+        if budget_s and time.time() - t0 > share:
+            break
+    t1 = time.time()
     for j, r in enumerate(gen.batch_requests(batch_count, SEED, offset)):
         db.append(time_request(r, reps))
         torch.cuda.empty_cache()
-        if verbose and (j + 1) % 25 == 0:
-            print(f"batch {j + 1}/{batch_count} timed, {time.time() - t0:.1f}s", flush=True)
+        if (j + 1) % 25 == 0:
+            save()
+            if verbose:
+                print(f"batch {j + 1}/{batch_count} timed, {time.time() - t0:.1f}s", flush=True)
+        if budget_s and time.time() - t1 > budget_s - share:
+            break
+    save()
     return db
 
 
@@ -212,11 +230,11 @@ def main():
     ap.add_argument("--offset", type=int, default=100000)
     ap.add_argument("--batches", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--budget", type=float, default=0.0, help="seconds (0: no limit)")
     ap.add_argument("--out", default="autotune_db.json")
     a = ap.parse_args()
-    db = build_db(a.count, a.offset, a.reps, batch_count=a.batches, verbose=True)
-    with open(a.out, "w") as f:
-        json.dump(db, f)
+    db = build_db(a.count, a.offset, a.reps, batch_count=a.batches, verbose=True, out=a.out,
+                  budget_s=a.budget)
     print(f"{len(db)} records -> {a.out}; all configurations agree: {all(r['agree'] for r in db)}")
 
 

@@ -157,9 +157,33 @@ def install(params: np.ndarray | None):
     check(lib().mela_costmodel_load(buf.ctypes.data))
 
 
+def predict_host(op: str, m: int, n: int, p: int, density: float, batch_count: int = 1,
+                 batch_log2_cells: float | None = None):
+    """The installed model's predicted log2 microseconds per configuration
+    (dict by name), evaluated on the host by the library; None without a model."""
+    y = (C.c_float * _lib.MLP_OUT)()
+    cnt = lib().mela_costmodel_predict(OPS[op], int(m), int(n), int(p), float(density), int(batch_count),
+                                       _mix(m, n, batch_log2_cells), y)
+    if cnt < 0:
+        return None
+    return {CONFIG_NAMES[op][i]: float(y[i]) for i in range(cnt)}
+
+
+def install_default():
+    """Put back the model the library loads with (costmodel.json), if any."""
+    install(load() if os.path.exists(DEFAULT_MODEL) else None)
+
+
 def choose(op: str, m: int, n: int, p: int, density: float, batch_count: int = 1,
-           batch_log2_cells: float | None = None) -> str:
-    """Configuration the installed model picks (name); the fixed rule without one."""
+           batch_log2_cells: float | None = None, among=None) -> str:
+    """Configuration the installed model picks (name) -- among the names in
+    `among` when given (e.g. the batch engines a matrix fits); the fixed
+    rule without a model."""
+    if among is not None:
+        y = predict_host(op, m, n, p, density, batch_count, batch_log2_cells)
+        if y is None:
+            return heuristic(op, m, n, p, density)
+        return min(among, key=lambda name: y[name])
     v = lib().mela_costmodel_choose(OPS[op], int(m), int(n), int(p), float(density), int(batch_count),
                                     _mix(m, n, batch_log2_cells))
     if v < 0:

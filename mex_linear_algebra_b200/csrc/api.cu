@@ -5,10 +5,12 @@
 // run every computation on the GPU: host arrays are copied in, packed,
 // processed and unpacked by kernels, and copied out.  Device entry points
 // are stream-ordered and never synchronise.
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "mela_common.cuh"
@@ -331,6 +333,151 @@ size_t gemm_workspace(int variant, i64 m, i64 k, i64 n)
 }
 
 // ---------------------------------------------------------------- host-matrix helpers
+namespace {
+// Host threads that copy a caller's (pageable) array into page-locked
+// staging memory in parallel: one copy thread saturates neither the host's
+// memory system nor the PCIe link.  Created on first use, never torn down.
+class CopyPool {
+public:
+    static CopyPool &get()
+    {
+        static CopyPool *p = new CopyPool();
+        return *p;
+    }
+    // dst[0, bytes) = src[0, bytes), split over the pool and the caller.
+    void copy(void *dst, const void *src, size_t bytes)
+    {
+        const int parts = (int)workers_.size() + 1;
+        if (bytes < ((size_t)1 << 20) || parts == 1) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        std::lock_guard<std::mutex> one_job(call_mu_);  // callers on other threads queue here
+        std::unique_lock<std::mutex> lk(mu_);
+        job_dst_ = (char *)dst;
+        job_src_ = (const char *)src;
+        job_bytes_ = bytes;
+        job_parts_ = parts;
+        pending_ = parts - 1;
+        ++gen_;
+        lk.unlock();
+        cv_.notify_all();
+        run_part(0);
+        lk.lock();
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+private:
+    CopyPool()
+    {
+        unsigned hw = std::thread::hardware_concurrency();
+        int n = hw >= 4 ? (int)(hw / 2) : 1;
+        if (n > 8) n = 8;
+        for (int i = 1; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
+        for (auto &t : workers_) t.detach();
+    }
+    void run_part(int i)
+    {
+        const size_t per = (job_bytes_ / job_parts_ + 63) & ~(size_t)63;
+        const size_t a = per * (size_t)i, b = a + per < job_bytes_ ? a + per : job_bytes_;
+        if (a < b) std::memcpy(job_dst_ + a, job_src_ + a, b - a);
+    }
+    void loop(int i)
+    {
+        unsigned long long seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            lk.unlock();
+            run_part(i);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex call_mu_, mu_;
+    std::condition_variable cv_, done_;
+    unsigned long long gen_ = 0;
+    int pending_ = 0, job_parts_ = 1;
+    char *job_dst_ = nullptr;
+    const char *job_src_ = nullptr;
+    size_t job_bytes_ = 0;
+};
+
+// Page-locked staging slots of the calling thread, reused across calls: a
+// slot is refilled once the upload that read it has completed.
+constexpr int kStageSlots = 3;
+constexpr size_t kStageBytes = (size_t)8 << 20;
+struct Staging {
+    void *slot[kStageSlots] = {};
+    cudaEvent_t read[kStageSlots] = {};  // the upload from the slot is done
+    cudaEvent_t fence = nullptr;         // the device staging buffer is allocated
+    bool ready = false;
+    bool failed = false;
+};
+thread_local Staging t_stage;
+
+bool staging_ready()
+{
+    Staging &S = t_stage;
+    if (S.ready) return true;
+    if (S.failed) return false;
+    for (int i = 0; i < kStageSlots; ++i) {
+        if (cudaMallocHost(&S.slot[i], kStageBytes) != cudaSuccess ||
+            cudaEventCreateWithFlags(&S.read[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            S.failed = true;
+            return false;
+        }
+    }
+    if (cudaEventCreateWithFlags(&S.fence, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        S.failed = true;
+        return false;
+    }
+    S.ready = true;
+    return true;
+}
+}  // namespace
+
+// Column blocks of the MATLAB array go through the page-locked slots: the
+// host copy of block b+1 (parallel memcpy) overlaps the upload of block b on
+// the upload stream, and each block is packed on s as soon as it has landed
+// (blocks are whole packed words: multiples of 64 columns).
+static mela_status upload_and_pack_blocks(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStream_t s,
+                                          DevBuf &staging, i64 cols_per_block)
+{
+    const i64 m = M->rows, n = M->cols;
+    const size_t esz = M->kind == MELA_KIND_DOUBLE ? 8 : 1;
+    mela_status st = staging.alloc((size_t)m * (size_t)n * esz, s);
+    if (st != MELA_OK) return st;
+    cudaStream_t sin = nullptr, sout = nullptr;
+    if ((st = copy_streams(&sin, &sout)) != MELA_OK) return st;
+    Staging &S = t_stage;
+    // the device staging buffer comes from s's pool: uploads wait for it
+    MELA_CUDA_TRY(cudaEventRecord(S.fence, s));
+    MELA_CUDA_TRY(cudaStreamWaitEvent(sin, S.fence, 0));
+    const char *src = (const char *)M->data;
+    char *dst = (char *)staging.p;
+    int slot = 0;
+    for (i64 j0 = 0; j0 < n; j0 += cols_per_block) {
+        const i64 nc = n - j0 < cols_per_block ? n - j0 : cols_per_block;
+        const size_t off = (size_t)j0 * (size_t)m * esz, bytes = (size_t)nc * (size_t)m * esz;
+        MELA_CUDA_TRY(cudaEventSynchronize(S.read[slot]));  // the slot's previous upload is done
+        CopyPool::get().copy(S.slot[slot], src + off, bytes);
+        MELA_CUDA_TRY(cudaMemcpyAsync(dst + off, S.slot[slot], bytes, cudaMemcpyHostToDevice, sin));
+        MELA_CUDA_TRY(cudaEventRecord(S.read[slot], sin));
+        MELA_CUDA_TRY(cudaStreamWaitEvent(s, S.read[slot], 0));
+        // the last block also writes the row padding words
+        const i64 words = j0 + nc >= n ? ld - j0 / 64 : words_of(nc);
+        if ((st = launch_pack_words(M->kind, m, nc, dst + off, dP + j0 / 64, ld, words, s)) != MELA_OK)
+            return st;
+        slot = (slot + 1) % kStageSlots;
+    }
+    return MELA_OK;
+}
+
 mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStream_t s,
                             DevBuf &staging)
 {
@@ -341,6 +488,10 @@ mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStre
     }
     const size_t esz = M->kind == MELA_KIND_DOUBLE ? 8 : 1;
     const size_t bytes = (size_t)m * (size_t)n * esz;
+    // blocks of whole packed words that fit a staging slot
+    const i64 cols_per_block = (i64)(kStageBytes / ((size_t)m * esz)) / 64 * 64;
+    if (bytes >= ((size_t)2 << 20) && cols_per_block >= 64 && staging_ready())
+        return upload_and_pack_blocks(M, dP, ld, s, staging, cols_per_block);
     mela_status st = staging.alloc(bytes, s);
     if (st != MELA_OK) return st;
     MELA_CUDA_TRY(cudaMemcpyAsync(staging.p, M->data, bytes, cudaMemcpyHostToDevice, s));

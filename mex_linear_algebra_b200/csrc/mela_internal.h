@@ -14,6 +14,10 @@ mela_status launch_rand_dense(u64 seed, u64 stream_id, i64 m, i64 n, u64 *out, i
 mela_status launch_rand_bernoulli(u64 seed, u64 stream_id, i64 m, i64 n, double density, u64 *out,
                                   i64 ld, cudaStream_t s);
 mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, cudaStream_t s);
+// The same, writing only the first out_words words of each packed row (the
+// words of a column block, for packing a matrix block by block).
+mela_status launch_pack_words(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, i64 out_words,
+                              cudaStream_t s);
 mela_status launch_unpack(const u64 *in, i64 ld, i64 m, i64 n, unsigned char *out, cudaStream_t s);
 mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *out, i64 ld_out,
                              cudaStream_t s);

@@ -316,6 +316,18 @@ extern "C" int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64
                             batch_log2_cells);
 }
 
+extern "C" int32_t mela_costmodel_predict(int32_t op, int64_t m, int64_t n, int64_t p, double density,
+                                          int64_t batch_count, double batch_log2_cells, float *y)
+{
+    const int nc = config_count(op);
+    float out[kOut];
+    if (nc <= 0 || !y ||
+        !costmodel_predict(op, (double)m, (double)n, (double)p, density, (double)batch_count, batch_log2_cells, out))
+        return -1;
+    for (int i = 0; i < nc; ++i) y[i] = out[i];
+    return nc;
+}
+
 extern "C" void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                                         int64_t batch_count, double batch_log2_cells, float *x)
 {

@@ -85,7 +85,7 @@ __device__ __forceinline__ u32 parity_of(unsigned char x) { return x != 0; }
 // so each load instruction reads 32 consecutive rows of one column.
 template <typename T>
 __global__ void __launch_bounds__(256) pack_kernel(const T *__restrict__ in, i64 m, i64 n,
-                                                   u64 *__restrict__ out, i64 ld)
+                                                   u64 *__restrict__ out, i64 ld, i64 out_words)
 {
     __shared__ u64 tile[32][9];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const T *__restrict__ in, i64
     __syncthreads();
     const int r = threadIdx.x >> 3, q = threadIdx.x & 7;
     const i64 orow = row0 + r, ow = (i64)blockIdx.y * 8 + q;
-    if (orow < m && ow < ld) out[orow * ld + ow] = tile[r][q];
+    if (orow < m && ow < out_words) out[orow * ld + ow] = tile[r][q];
 }
 
 // ---------------------------------------------------------------- unpack
@@ -336,15 +336,21 @@ mela_status launch_transpose(const u64 *in, i64 ld_in, i64 rows, i64 cols, u64 *
 
 mela_status launch_pack(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, cudaStream_t s)
 {
+    return launch_pack_words(kind, m, n, in, out, ld, ld, s);
+}
+
+mela_status launch_pack_words(int kind, i64 m, i64 n, const void *in, u64 *out, i64 ld, i64 out_words,
+                              cudaStream_t s)
+{
     if (m <= 0) return MELA_OK;
-    i64 wgroups = (ld + 7) / 8;
+    i64 wgroups = (out_words + 7) / 8;
     if (wgroups == 0) return MELA_OK;
     if (mela_status st = check_grid_yz(wgroups, 1, "pack"); st != MELA_OK) return st;
     dim3 grid((unsigned)((m + 31) / 32), (unsigned)wgroups);
     if (kind == MELA_KIND_DOUBLE)
-        pack_kernel<double><<<grid, 256, 0, s>>>((const double *)in, m, n, out, ld);
+        pack_kernel<double><<<grid, 256, 0, s>>>((const double *)in, m, n, out, ld, out_words);
     else
-        pack_kernel<unsigned char><<<grid, 256, 0, s>>>((const unsigned char *)in, m, n, out, ld);
+        pack_kernel<unsigned char><<<grid, 256, 0, s>>>((const unsigned char *)in, m, n, out, ld, out_words);
     MELA_LAUNCH_CHECK("pack_kernel");
     return MELA_OK;
 }

@@ -68,3 +68,39 @@ def shard_batch(shapes, world_size: int, rank: int) -> np.ndarray:
         owner[i] = r
         load[r] += cost[i]
     return np.nonzero(owner == rank)[0]
+
+
+def gather_objects(ws: int, obj):
+    """Every rank's `obj`, in rank order, on every rank (host objects)."""
+    if ws == 1:
+        return [obj]
+    import torch.distributed as dist
+    out = [None] * ws
+    dist.all_gather_object(out, obj)
+    return out
+
+
+def run_sharded(shapes, ws: int, rank: int, compute):
+    """One batch split over the ranks with no data exchange: rank r runs
+    ``compute(indices)`` on the matrices ``shard_batch`` gives it (the
+    indices into `shapes`) and returns a dict {index: result}; the results
+    are gathered on the host of every rank.  Returns (merged results, the
+    indices each rank ran).  Raises if a matrix was computed by no rank or
+    by two."""
+    mine = shard_batch(shapes, ws, rank)
+    local = compute(mine)
+    parts = gather_objects(ws, (mine.tolist(), local))
+    merged, owners = {}, []
+    for idx, res in parts:
+        owners.append(idx)
+        for i in idx:
+            if i in merged:
+                raise RuntimeError(f"matrix {i} computed by two ranks")
+            if i not in res:
+                raise RuntimeError(f"matrix {i} has no result from its rank")
+            merged[i] = res[i]
+    missing = set(range(len(np.asarray(shapes).reshape(-1, 2)))) - set(merged)
+    if missing:
+        raise RuntimeError(f"{len(missing)} matrices computed by no rank")
+    return merged, owners
+

@@ -64,7 +64,7 @@ def test_auto_through_every_product_configuration(cuda):
             got = to_host(D.matmul(to_dev(A), to_dev(B), m, k, n, variant="auto"))
             assert np.array_equal(valid_words(got, n), want), name
     finally:
-        costmodel.install(None)
+        costmodel.install_default()
 
 
 @pytest.mark.parametrize("op", ["rank", "null"])
@@ -100,7 +100,7 @@ def test_auto_through_every_elimination_configuration(cuda, op):
                 Zt = dev_null(M, m, n, r, pv, to_host(prow)[:r].astype(np.int64))
                 assert np.array_equal(valid_words(Zt, n), want_Z), name
     finally:
-        costmodel.install(None)
+        costmodel.install_default()
 
 
 def test_learned_batch_engines(cuda):
@@ -137,4 +137,52 @@ def test_learned_batch_engines(cuda):
                 assert st["cta"] == len(mats)
             plan.close()
     finally:
-        costmodel.install(None)
+        costmodel.install_default()
+
+
+def test_trained_model_gains_live(cuda):
+    """The library's compiled-in model against its fixed rule, timed live on
+    held-out product requests of the mixed stream where the rule stays on
+    the plain form because one dimension is under 1024 (the model sends them
+    to the FP4 tensor cores on single CTAs): AUTO with the model, including
+    its device density measurement, is faster in total, and bit-exact."""
+    import torch
+    from mex_linear_algebra_b200 import _lib, costmodel, device as D
+    L = _lib.lib()
+    assert L.mela_costmodel_choose(_lib.OP_MATMUL, 775, 6198, 6701, 0.1, 1, 22.2) >= 0, \
+        "the library was built without its trained model"
+    params = costmodel.load()
+    reqs = [(775, 6198, 6701), (5695, 5715, 962), (6592, 824, 4978), (3020, 7212, 935)]
+
+    def med(fn, reps=7):
+        fn()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    t_model = t_rule = 0.0
+    try:
+        for (m, k, n) in reqs:
+            A, B = D.rand_dense(96, 0, m, k), D.rand_dense(96, 1, k, n)
+            out = {}
+            for label, model in (("model", params), ("rule", None)):
+                costmodel.install(model)
+                C = D.empty_packed(m, n)
+                wsb = D.matmul_workspace("auto", m, k, n)
+                ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+                t = med(lambda: D.matmul(A, B, m, k, n, variant="auto", out=C, workspace=ws))
+                out[label] = C.clone()
+                if label == "model":
+                    t_model += t
+                else:
+                    t_rule += t
+            assert torch.equal(out["model"], out["rule"]), (m, k, n)
+    finally:
+        costmodel.install_default()
+    assert t_model < 0.8 * t_rule, (t_model, t_rule)
