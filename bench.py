@@ -934,6 +934,32 @@ def batch_only(lo: int, hi: int, logical: bool = False, reps: int = 3):
     plan.close()
 
 
+def form_only(form: str, reps: int = 3):
+    """Profiling aid: C = A*B at the --size cube (seed 1) by one product form,
+    `reps` timed calls after a warm-up; prints the median time and rate."""
+    import torch
+    from mex_linear_algebra_b200 import _lib, device as D
+    v = _lib.GEMM_VARIANTS[form]
+    A = D.rand_dense(SEED, 0, M, K)
+    B = D.rand_dense(SEED, 1, K, N)
+    C = D.empty_packed(M, N)
+    wsb = D.matmul_workspace(v, M, K, N)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    D.matmul(A, B, M, K, N, variant=v, out=C, workspace=ws)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        D.matmul(A, B, M, K, N, variant=v, out=C, workspace=ws)
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ts.sort()
+    ms = ts[len(ts) // 2]
+    print(json.dumps({"form": form, "size": M, "ms": round(ms, 3), "tbitops": round(BITOPS / (ms * 1e-3) / 1e12, 1)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -956,8 +982,12 @@ def main():
                          "(packed input, no graph) and print its time, nothing else")
     ap.add_argument("--batch-logical", action="store_true",
                     help="with --batch-only: start from the MATLAB logical input instead")
+    ap.add_argument("--form-only", choices=["plain", "m4ri", "tc", "tc_fp4"],
+                    help="profiling aid: time one product form at the --size cube, nothing else")
     args = ap.parse_args()
     set_size(args.size)
+    if args.form_only:
+        return form_only(args.form_only)
     if args.elim_only:
         return elim_only()
     if args.batch_only:

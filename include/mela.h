@@ -416,15 +416,20 @@ int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, doubl
  * that count, or -1 when no model is installed. */
 int32_t mela_costmodel_predict(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                                int64_t batch_count, double batch_log2_cells, float *y);
+/* The variant argument the calling thread's last AUTO call resolved to (-1
+ * before any), and in *density the density it measured on the device for
+ * the choice, or a negative value when none was needed: the density is read
+ * back only when the model's choice differs across densities 0.001 .. 0.5. */
+int32_t mela_dispatch_last(double *density);
 /* The MELA_MLP_IN input features of a request. */
 void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                              int64_t batch_count, double batch_log2_cells, float *x);
 /* Number of ones of the packed m x n device matrix into *d_count (device),
  * stream-ordered: the density the dispatcher feeds the model.  The AUTO
  * variants of mela_dev_matmul / mela_dev_rank / mela_dev_rref measure it
- * this way when a model is installed -- which waits for the stream (the
- * count is read back) unless the stream is being captured, where 0.5 is
- * assumed. */
+ * this way when a model is installed and its choice depends on the density
+ * -- which waits for the stream (the count is read back) unless the stream
+ * is being captured, where 0.5 is assumed. */
 mela_status mela_dev_popcount(const uint64_t *dM, int64_t ld, int64_t m, int64_t n, int64_t *d_count,
                               void *stream);
 

@@ -157,6 +157,17 @@ mela_status launch_popcount(const u64 *M, i64 ld, i64 m, i64 n, long long *d_cou
     return MELA_OK;
 }
 
+// The calling thread's counter for density read-backs: one device word and
+// one page-locked host word per device, allocated on first use.
+namespace {
+struct DensitySlot {
+    long long *d = nullptr;
+    long long *h = nullptr;
+    bool failed = false;
+};
+thread_local DensitySlot t_density[64];
+}  // namespace
+
 double measure_density(const u64 *M, i64 ld, i64 m, i64 n, cudaStream_t s)
 {
     if (m <= 0 || n <= 0 || !M) return 0.5;
@@ -165,16 +176,61 @@ double measure_density(const u64 *M, i64 ld, i64 m, i64 n, cudaStream_t s)
         cudaGetLastError();
         return 0.5;  // no read-back while a graph is being captured
     }
-    DevBuf cnt;
-    if (cnt.alloc(sizeof(long long), s) != MELA_OK) return 0.5;
-    long long h = 0;
-    if (launch_popcount(M, ld, m, n, (long long *)cnt.p, s) != MELA_OK ||
-        cudaMemcpyAsync(&h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0.5;
+    DensitySlot &S = t_density[dev];
+    if (!S.d && !S.failed) {
+        if (cudaMalloc((void **)&S.d, sizeof(long long)) != cudaSuccess ||
+            cudaMallocHost((void **)&S.h, sizeof(long long)) != cudaSuccess) {
+            cudaGetLastError();
+            S.failed = true;
+        }
+    }
+    if (S.failed) return 0.5;
+    if (launch_popcount(M, ld, m, n, S.d, s) != MELA_OK ||
+        cudaMemcpyAsync(S.h, S.d, sizeof(long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         return 0.5;
     }
-    return (double)h / ((double)m * (double)n);
+    return (double)*S.h / ((double)m * (double)n);
+}
+
+// The calling thread's last AUTO resolution (mela_dispatch_last).
+namespace {
+thread_local int32_t t_last_variant = -1;
+thread_local double t_last_density = -1.0;
+}  // namespace
+
+static int32_t remember(int32_t v, double density)
+{
+    t_last_variant = v;
+    t_last_density = density;
+    return v;
+}
+
+// The model's choice for a request whose density is not known yet: the
+// choices at densities spanning the model's range are compared first, and
+// the density is measured on the device (a popcount and a read-back that
+// waits for the stream) only when they differ.
+static int choose_measuring(int op, double m, double n, double p, double cells,
+                            const u64 *M, i64 ld, i64 rows, i64 cols, cudaStream_t s)
+{
+    static const double probe[] = {0.001, 0.01, 0.1, 0.5};
+    const double lc = std::log2(cells > 1 ? cells : 1);
+    int first = -1;
+    bool same = true;
+    for (double d : probe) {
+        const int c = costmodel_choose(op, m, n, p, d, 1, lc);
+        if (c < 0) return -1;
+        if (first < 0) first = c;
+        else if (c != first) same = false;
+    }
+    t_last_density = -1.0;
+    if (same) return first;
+    const double d = measure_density(M, ld, rows, cols, s);
+    t_last_density = d;
+    return costmodel_choose(op, m, n, p, d, 1, lc);
 }
 
 // ---------------------------------------------------------------- choices
@@ -182,18 +238,17 @@ int32_t resolve_gemm_variant(int32_t variant, const u64 *A, i64 lda, i64 m, i64 
 {
     if (MELA_VARIANT_BASE(variant) != MELA_GEMM_AUTO) return variant;
     if (costmodel_loaded() && m > 0 && n > 0 && k > 0) {
-        const double d = measure_density(A, lda, m, k, s);
-        const int c = costmodel_choose(MELA_OP_MATMUL, (double)m, (double)k, (double)n, d, 1,
-                                       std::log2((double)m * (double)k));
+        const int c = choose_measuring(MELA_OP_MATMUL, (double)m, (double)k, (double)n, (double)m * (double)k,
+                                       A, lda, m, k, s);
         if (c >= 0) {
             int32_t v = config_variant(MELA_OP_MATMUL, c);
             // the FP4 form's f32 sums are exact below 2^24: past 2^23 terms use INT8
             if (MELA_VARIANT_BASE(v) == MELA_GEMM_TC_FP4 && k >= (1LL << 23))
                 v = MELA_GEMM_TC | (v & ~0xff);
-            return v;
+            return remember(v, t_last_density);
         }
     }
-    return fixed_gemm_variant(m, k, n);
+    return remember(fixed_gemm_variant(m, k, n), -1.0);
 }
 
 int32_t fixed_gemm_variant(i64 m, i64 k, i64 n)
@@ -209,12 +264,11 @@ int32_t resolve_elim_variant(int32_t variant, const u64 *M, i64 ld, i64 m, i64 n
 {
     if (MELA_VARIANT_BASE(variant) != MELA_ELIM_AUTO) return variant;
     if (costmodel_loaded() && m > 0 && n > 0) {
-        const double d = measure_density(M, ld, m, n, s);
-        const int c = costmodel_choose(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0, d, 1,
-                                       std::log2((double)m * (double)n));
-        if (c >= 0) return config_variant(MELA_OP_RANK, c);
+        const int c = choose_measuring(rref ? MELA_OP_NULL : MELA_OP_RANK, (double)m, (double)n, 0.0,
+                                       (double)m * (double)n, M, ld, m, n, s);
+        if (c >= 0) return remember(config_variant(MELA_OP_RANK, c), t_last_density);
     }
-    return fixed_elim_variant(m, n);
+    return remember(fixed_elim_variant(m, n), -1.0);
 }
 
 int32_t fixed_elim_variant(i64 m, i64 n)
@@ -228,6 +282,12 @@ int32_t fixed_elim_variant(i64 m, i64 n)
 using namespace mela;
 
 extern "C" int32_t mela_costmodel_config_count(int32_t op) { return config_count(op); }
+
+extern "C" int32_t mela_dispatch_last(double *density)
+{
+    if (density) *density = t_last_density;
+    return t_last_variant;
+}
 
 extern "C" int32_t mela_costmodel_config(int32_t op, int32_t index) { return config_variant(op, index); }
 

@@ -478,6 +478,28 @@ mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 
     return make_map(map, base, rows, kp, box_rows);
 }
 
+mela_status make_u64_rows_map(CUtensorMap *map, const u64 *base, i64 rows, i64 words, i64 ld, int box_words,
+                              int box_rows)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled unavailable");
+        return MELA_ERR_CUDA;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)words, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    cuuint32_t box[2] = {(cuuint32_t)box_words, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (packed rows) failed (%d)", (int)r);
+        return MELA_ERR_CUDA;
+    }
+    return MELA_OK;
+}
+
 // CTA pairs are used whenever the padded row count allows (mp % 256 == 0),
 // unless the tile choice asks for single CTAs (tile 1) or, for the default
 // choice, MELA_TC_PAIR=0 is set in the environment.

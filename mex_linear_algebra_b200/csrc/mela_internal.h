@@ -47,6 +47,11 @@ mela_status launch_gemm_tc(const unsigned char *A8, const unsigned char *Bt8, i6
 // TMA map of a K-major byte matrix rows x kp (row pitch kp bytes): boxes of
 // 128 bytes x box_rows rows with 128-byte swizzle, as the tcgen05 kernels read them.
 mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 rows, i64 kp, int box_rows);
+// TMA map of packed rows (rows x words uint64, row pitch ld words; ld * 8 must
+// be a multiple of 16 and base 16-byte aligned): boxes of box_words x box_rows,
+// no swizzle, zeros read past the edges.
+mela_status make_u64_rows_map(CUtensorMap *map, const u64 *base, i64 rows, i64 words, i64 ld, int box_words,
+                              int box_rows);
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
                              i64 m, i64 k, i64 n, cudaStream_t s);
 

@@ -186,3 +186,66 @@ def test_trained_model_gains_live(cuda):
     finally:
         costmodel.install_default()
     assert t_model < 0.8 * t_rule, (t_model, t_rule)
+
+
+def _density_model(op, dense_cfg, sparse_cfg):
+    """Weights whose choice flips with the density feature x3 = log10(d)/3 + 1:
+    y[dense_cfg] = 10 - 20 * x3, y[sparse_cfg] = 4, the others 10 -- dense_cfg
+    above d = 10^-2.1 (about 0.008), sparse_cfg below."""
+    from mex_linear_algebra_b200 import _lib
+    IN, H1, H2, OUT = _lib.MLP_IN, _lib.MLP_H1, _lib.MLP_H2, _lib.MLP_OUT
+    p = np.zeros(_lib.MLP_PARAMS, dtype=np.float32)
+    oW1, ob1 = 0, IN * H1
+    oW2, ob2 = ob1 + H1, ob1 + H1 + H1 * H2
+    oW3 = ob2 + H2
+    ob3 = oW3 + H2 * OUT
+    p[oW1 + 3 * H1 + 0] = 1.0         # h1[0] = relu(x3)
+    p[oW2 + 0 * H2 + 0] = 1.0         # h2[0] = relu(h1[0])
+    p[oW3 + 0 * OUT + dense_cfg] = -20.0
+    p[ob3:ob3 + OUT] = 10.0
+    p[ob3 + sparse_cfg] = 4.0
+    return p
+
+
+def test_auto_measures_density_when_it_matters(cuda):
+    """With a model whose choice depends on the density, the AUTO call
+    counts the input's ones on the device and follows the count: dense
+    input -> one configuration, sparse input -> the other (read back with
+    mela_dispatch_last), with the oracle's results either way."""
+    import ctypes as C
+    import torch
+    from mex_linear_algebra_b200 import _lib, costmodel
+    L = _lib.lib()
+    names = costmodel.CONFIG_NAMES["rank"]
+    dense_i, sparse_i = names.index("m4ri_k8"), names.index("tc")
+    m, n = 600, 1300
+    s = torch.cuda.current_stream().cuda_stream
+    try:
+        costmodel.install(_density_model("rank", dense_i, sparse_i))
+        for dens, want_i in ((0.5, dense_i), (0.002, sparse_i)):
+            from mex_linear_algebra_b200 import gen
+            P = gen.sparse_packed(97, 0, m, n, dens)
+            M = to_dev(P)
+            rank = torch.zeros(1, dtype=torch.int64, device="cuda")
+            piv = torch.empty(m, dtype=torch.int64, device="cuda")
+            prow = torch.empty(m, dtype=torch.int64, device="cuda")
+            wsb = L.mela_elim_workspace_size(m, n)
+            ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+            _lib.check(L.mela_dev_rank(_lib.ELIM_AUTO, M.data_ptr(), M.shape[1], m, n, rank.data_ptr(),
+                                       piv.data_ptr(), prow.data_ptr(), ws.data_ptr(), wsb, s))
+            d = C.c_double(0)
+            v = L.mela_dispatch_last(C.byref(d))
+            ones = int(np.unpackbits(P.view(np.uint8)).sum())
+            assert abs(d.value - ones / (m * n)) < 1e-12           # measured on the device
+            assert v == costmodel.config_codes("rank")[want_i], (dens, hex(v))
+            assert int(rank.item()) == O.rank(P, m, n)
+        # a model whose choice does not depend on the density: nothing is measured
+        costmodel.install(_forcing_model(10, dense_i))
+        M = to_dev(gen.sparse_packed(97, 1, m, n, 0.3))
+        _lib.check(L.mela_dev_rank(_lib.ELIM_AUTO, M.data_ptr(), M.shape[1], m, n, rank.data_ptr(),
+                                   piv.data_ptr(), prow.data_ptr(), ws.data_ptr(), wsb, s))
+        d = C.c_double(0)
+        assert L.mela_dispatch_last(C.byref(d)) == costmodel.config_codes("rank")[dense_i]
+        assert d.value < 0
+    finally:
+        costmodel.install_default()
