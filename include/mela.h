@@ -96,7 +96,9 @@ typedef enum {
  *                      2: 1024 (default), 3: 4096.
  *                      MELA_GEMM_TC / _TC_FP4: t = 1: one CTA per 128 x 256
  *                      tile; 2: CTA pairs per 256 x 256 tile (the default
- *                      where the padded row count allows). */
+ *                      where the padded row count allows).
+ *                      MELA_GEMM_M4RI: t = 1: 8 warps of 64 rows per CTA;
+ *                      2: 16 warps of 32 rows (the default). */
 #define MELA_VARIANT_BASE(v) ((int32_t)(v) & 0xff)
 #define MELA_TUNE_K(k) ((int32_t)(k) << 8)
 #define MELA_TUNE_TILE(t) ((int32_t)(t) << 12)
@@ -110,6 +112,18 @@ const char *mela_status_string(mela_status s);
 const char *mela_last_error(void);
 /* Device-side error bits (timeouts of bounded waits); `clear` resets them. */
 mela_status mela_device_error_flags(uint32_t *flags, int clear);
+/* Host-array uploads of the calling thread since the last reset: bytes sent
+ * through the page-locked staging slots (column blocks of 2 MiB and larger
+ * arrays, host copies overlapping the uploads) and bytes copied directly,
+ * with the host time spent copying into the slots and waiting for a slot. */
+typedef struct {
+    int64_t blocked_bytes;
+    int64_t direct_bytes;
+    int64_t blocks;
+    double host_copy_us;
+    double slot_wait_us;
+} mela_upload_stats;
+void mela_upload_stats_get(mela_upload_stats *out, int reset);
 /* Diagnostic of the failure path (no reference counterpart): one kernel whose
  * wait nothing will satisfy -- kind 0 a device flag, kind 1 an mbarrier with
  * tensor memory held -- runs out after limit_ns (1 us .. 1 s), sets the

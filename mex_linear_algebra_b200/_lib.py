@@ -55,6 +55,11 @@ class HostMatrix(C.Structure):
                 ("cols", C.c_int64), ("data", C.c_void_p)]
 
 
+class UploadStats(C.Structure):
+    _fields_ = [("blocked_bytes", C.c_int64), ("direct_bytes", C.c_int64), ("blocks", C.c_int64),
+                ("host_copy_us", C.c_double), ("slot_wait_us", C.c_double)]
+
+
 class HostCsc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("rows", C.c_int64), ("cols", C.c_int64),
                 ("colptr", C.c_void_p), ("rowidx", C.c_void_p), ("values", C.c_void_p)]
@@ -69,6 +74,7 @@ SIGNATURES = {
     "mela_last_error": (C.c_char_p, []),
     "mela_device_error_flags": (_st, [C.POINTER(_u32), C.c_int]),
     "mela_diag_wait_timeout": (_st, [_i32, _u64, _vp, _i32, _vp]),
+    "mela_upload_stats_get": (None, [C.POINTER(UploadStats), C.c_int]),
     "mela_matmul_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
     "mela_matmul_m4ri": (_st, [C.POINTER(HostMatrix), C.POINTER(HostMatrix), _vp]),
     "mela_rank_gf2": (_st, [C.POINTER(HostMatrix), C.POINTER(C.c_double)]),

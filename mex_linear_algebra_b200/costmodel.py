@@ -36,7 +36,7 @@ OPS = {"rank": _lib.OP_RANK, "null": _lib.OP_NULL, "matmul": _lib.OP_MATMUL, "ba
 ELIM_CONFIGS = ("plain", "m4ri_k4", "m4ri_k6", "m4ri_k7", "m4ri_k8", "m4ri_k8_rt256", "m4ri_k9_rt4096",
                 "m4ri_k10_rt4096", "fused", "tc")
 CONFIG_NAMES = {"rank": ELIM_CONFIGS, "null": ELIM_CONFIGS,
-                "matmul": ("plain", "m4ri", "tc_pair", "tc_single", "tc_fp4_pair", "tc_fp4_single"),
+                "matmul": ("plain", "m4ri", "m4ri_w8", "tc_pair", "tc_single", "tc_fp4_pair", "tc_fp4_single"),
                 "batch": ("cta", "group", "warp")}
 # kept for callers of the earlier name
 VARIANT_NAMES = CONFIG_NAMES

@@ -5,6 +5,7 @@
 // run every computation on the GPU: host arrays are copied in, packed,
 // processed and unpacked by kernels, and copied out.  Device entry points
 // are stream-ordered and never synchronise.
+#include <chrono>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -185,7 +186,7 @@ static i64 round_up(i64 x, i64 a) { return (x + a - 1) / a * a; }
 // workspace layout for each variant
 struct GemmPlan {
     int variant;          // base variant
-    int tc_tile;          // tensor-core tile choice (0 default, 1 single CTAs, 2 CTA pairs)
+    int tc_tile;          // tile choice: tensor cores 1 single CTAs / 2 CTA pairs; M4RI 1 = 8 warps
     i64 ldbt;             // packed Bt row pitch (words)
     size_t bt_bytes;      // packed Bt
     i64 mp, np, kp;       // padded byte-operand shape (tensor cores)
@@ -303,7 +304,7 @@ mela_status gemm_run(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, 
             return MELA_ERR_UNSUPPORTED;
         }
         return launch_gemm_tc(b.A8, b.B8, p.mp, p.np, p.kp, C, ldc, m, n, s, true, p.tc_tile);
-    case MELA_GEMM_M4RI: return launch_gemm_m4ri(A, lda, B, ldb, C, ldc, m, k, n, s);
+    case MELA_GEMM_M4RI: return launch_gemm_m4ri(A, lda, B, ldb, C, ldc, m, k, n, s, p.tc_tile);
     default:
         set_error("unknown product variant %d", p.variant);
         return MELA_ERR_INVALID;
@@ -417,6 +418,12 @@ struct Staging {
     bool failed = false;
 };
 thread_local Staging t_stage;
+thread_local mela_upload_stats t_upload_stats;
+
+double now_us()
+{
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 bool staging_ready()
 {
@@ -464,8 +471,14 @@ static mela_status upload_and_pack_blocks(const mela_host_matrix *M, u64 *dP, i6
     for (i64 j0 = 0; j0 < n; j0 += cols_per_block) {
         const i64 nc = n - j0 < cols_per_block ? n - j0 : cols_per_block;
         const size_t off = (size_t)j0 * (size_t)m * esz, bytes = (size_t)nc * (size_t)m * esz;
+        const double t0 = now_us();
         MELA_CUDA_TRY(cudaEventSynchronize(S.read[slot]));  // the slot's previous upload is done
+        const double t1 = now_us();
         CopyPool::get().copy(S.slot[slot], src + off, bytes);
+        t_upload_stats.slot_wait_us += t1 - t0;
+        t_upload_stats.host_copy_us += now_us() - t1;
+        t_upload_stats.blocked_bytes += (int64_t)bytes;
+        t_upload_stats.blocks += 1;
         MELA_CUDA_TRY(cudaMemcpyAsync(dst + off, S.slot[slot], bytes, cudaMemcpyHostToDevice, sin));
         MELA_CUDA_TRY(cudaEventRecord(S.read[slot], sin));
         MELA_CUDA_TRY(cudaStreamWaitEvent(s, S.read[slot], 0));
@@ -495,6 +508,7 @@ mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStre
     mela_status st = staging.alloc(bytes, s);
     if (st != MELA_OK) return st;
     MELA_CUDA_TRY(cudaMemcpyAsync(staging.p, M->data, bytes, cudaMemcpyHostToDevice, s));
+    t_upload_stats.direct_bytes += (int64_t)bytes;
     return launch_pack(M->kind, m, n, staging.p, dP, ld, s);
 }
 
@@ -504,6 +518,12 @@ mela_status upload_and_pack(const mela_host_matrix *M, u64 *dP, i64 ld, cudaStre
 using namespace mela;
 
 extern "C" int mela_version(void) { return 10000; }
+
+extern "C" void mela_upload_stats_get(mela_upload_stats *out, int reset)
+{
+    if (out) *out = t_upload_stats;
+    if (reset) t_upload_stats = mela_upload_stats{};
+}
 
 extern "C" const char *mela_status_string(mela_status s)
 {

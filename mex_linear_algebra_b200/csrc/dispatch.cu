@@ -54,7 +54,8 @@ bool decode_gemm_variant(int32_t v, Tuning *t)
     if (base == MELA_GEMM_M4RI) {
         if (k && k != 8) return false;
         r.k = 8;
-        if (tile) return false;
+        if (tile > 2) return false;
+        r.tc_tile = tile;  // 1: 8 warps of 64 rows; 0 / 2: 16 warps of 32 rows
     } else if (base == MELA_GEMM_TC || base == MELA_GEMM_TC_FP4) {
         if (k || tile > 2) return false;
         r.tc_tile = tile;
@@ -70,8 +71,8 @@ bool decode_gemm_variant(int32_t v, Tuning *t)
 // over M4RI k = 4, 6, 7, 8 (with 1024-row update tiles), k = 8 with 256-row
 // tiles (more CTAs for short matrices), k = 9 and 10 with 4096-row tiles
 // (their larger tables pay off over more rows), the single-CTA form and the
-// tensor-core windows.  Products: plain, Four-Russians, and each tensor-core
-// form on CTA pairs and on single CTAs.  Batches: the engine per matrix.
+// tensor-core windows.  Products: plain, Four-Russians (16 warps of 32 rows
+// or 8 of 64), and each tensor-core form on CTA pairs and on single CTAs.  Batches: the engine per matrix.
 static const int32_t kElimConfigs[] = {
     MELA_ELIM_PLAIN,
     MELA_ELIM_M4RI_K4,
@@ -87,6 +88,7 @@ static const int32_t kElimConfigs[] = {
 static const int32_t kGemmConfigs[] = {
     MELA_GEMM_PLAIN,
     MELA_GEMM_M4RI,
+    MELA_GEMM_M4RI | MELA_TUNE_TILE(1),
     MELA_GEMM_TC | MELA_TUNE_TILE(2),
     MELA_GEMM_TC | MELA_TUNE_TILE(1),
     MELA_GEMM_TC_FP4 | MELA_TUNE_TILE(2),
@@ -209,25 +211,41 @@ static int32_t remember(int32_t v, double density)
     return v;
 }
 
-// The model's choice for a request whose density is not known yet: the
-// choices at densities spanning the model's range are compared first, and
-// the density is measured on the device (a popcount and a read-back that
-// waits for the stream) only when they differ.
+// The model's choice for a request whose density is not known yet.  The
+// model is evaluated at densities spanning its range first.  The density is
+// measured on the device (a popcount and a read-back that waits for the
+// stream, about 15 us) only when that can pay: when no single configuration
+// is predicted within kMeasureCostUs of the best at every probed density.
+// Otherwise that configuration (the one whose worst predicted loss is
+// smallest) is taken as it is.
+constexpr double kMeasureCostUs = 15.0;
+
 static int choose_measuring(int op, double m, double n, double p, double cells,
                             const u64 *M, i64 ld, i64 rows, i64 cols, cudaStream_t s)
 {
     static const double probe[] = {0.001, 0.01, 0.1, 0.5};
+    constexpr int kProbes = 4;
     const double lc = std::log2(cells > 1 ? cells : 1);
-    int first = -1;
-    bool same = true;
-    for (double d : probe) {
-        const int c = costmodel_choose(op, m, n, p, d, 1, lc);
-        if (c < 0) return -1;
-        if (first < 0) first = c;
-        else if (c != first) same = false;
+    const int nc = config_count(op);
+    float y[kProbes][MELA_MLP_OUT];
+    double best[kProbes];
+    for (int d = 0; d < kProbes; ++d) {
+        if (!costmodel_predict(op, m, n, p, probe[d], 1, lc, y[d])) return -1;
+        best[d] = 1e300;
+        for (int c = 0; c < nc; ++c) best[d] = std::fmin(best[d], std::exp2((double)y[d][c]));
+    }
+    int pick = 0;
+    double pick_loss = 1e300;
+    for (int c = 0; c < nc; ++c) {
+        double loss = 0;
+        for (int d = 0; d < kProbes; ++d) loss = std::fmax(loss, std::exp2((double)y[d][c]) - best[d]);
+        if (loss < pick_loss) {
+            pick_loss = loss;
+            pick = c;
+        }
     }
     t_last_density = -1.0;
-    if (same) return first;
+    if (pick_loss <= kMeasureCostUs) return pick;
     const double d = measure_density(M, ld, rows, cols, s);
     t_last_density = d;
     return costmodel_choose(op, m, n, p, d, 1, lc);

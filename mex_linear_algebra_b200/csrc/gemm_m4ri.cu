@@ -6,10 +6,11 @@
 // selected by its 8 bits of A.
 //
 // GPU organisation: a CTA owns a 512-row x 2048-column block of C; lane l of
-// every warp holds 64-bit column word l of the block, warp w the rows
-// 64w .. 64w+63 (64 accumulators of 64 bits).  K advances 16 bits per stage:
-// the 8 warps build the stage's two tables (2 strips x 256 entries x 32
-// words = 128 KB of shared memory), 64 entries each in Gray-code order --
+// every warp holds 64-bit column word l of the block; 16 warps own 32 rows
+// each (the default tile), or 8 warps 64 rows each (tile 1: fewer, fatter
+// warps).  K advances 16 bits per stage: the warps build the stage's two
+// tables (2 strips x 256 entries x 32 words = 128 KB of shared memory), an
+// equal share of the entries each in Gray-code order --
 // one 64-bit XOR and one store per entry --, then every row looks up its two
 // entries: the 32 lanes read one entry's 256 contiguous bytes (two
 // conflict-free wavefronts), the row's 16 index bits come from the lane that
@@ -33,32 +34,30 @@ namespace mela {
 
 namespace {
 __host__ __device__ constexpr int ctz_c(int x) { return (x & 1) ? 0 : 1 + ctz_c(x >> 1); }
-constexpr int M4_WARPS = 8;
-constexpr int M4_ROWS_PER_WARP = 64;
-constexpr int M4_CTA_ROWS = M4_WARPS * M4_ROWS_PER_WARP;  // 512
+constexpr int M4_CTA_ROWS = 512;                            // rows of C per CTA (8 or 16 warps)
 constexpr int M4_CTA_WORDS = 32;                            // 64-bit column words per CTA (2048 columns)
 constexpr int M4_STRIPS = 2;                                // 8-row strips of B per stage (16 bits of K)
 constexpr int M4_SMEM_BYTES = M4_STRIPS * 256 * M4_CTA_WORDS * 8;  // 128 KB
 
-// Steps J.. of a 64-entry Gray-code walk from position i0 (a multiple of 64):
+// Steps J.. of an E-entry Gray-code walk from position i0 (a multiple of E):
 // store the running XOR at entry g(i) = i ^ (i >> 1), then add the B row
 // whose bit flips next (bit ctz(i + 1) = ctz(J + 1), a constant here).
-template <int J>
+template <int J, int E>
 __device__ __forceinline__ void gray_walk(u64 *Ts, int i0, u64 &val, const u64 (&bv)[8])
 {
-    if constexpr (J < 64) {
+    if constexpr (J < E) {
         const int i = i0 + J;
         Ts[(i ^ (i >> 1)) * M4_CTA_WORDS] = val;
-        if constexpr (J < 63) val ^= bv[ctz_c(J + 1)];
-        gray_walk<J + 1>(Ts, i0, val, bv);
+        if constexpr (J < E - 1) val ^= bv[ctz_c(J + 1)];
+        gray_walk<J + 1, E>(Ts, i0, val, bv);
     }
 }
 }  // namespace
 
 constexpr int M4_BTILE_WORDS = 16 * M4_CTA_WORDS;  // one stage's rows of B (4 KB)
 
-template <bool kTma>
-__global__ void __launch_bounds__(256, 1)
+template <int WARPS, bool kTma>
+__global__ void __launch_bounds__(WARPS * 32, 1)
 gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, i64 ldb,
                  u64 *__restrict__ C, i64 ldc, i64 m, i64 k, i64 n, const __grid_constant__ CUtensorMap bmap,
                  u32 *err)
@@ -66,14 +65,17 @@ gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, 
     extern __shared__ __align__(128) u64 T[];  // [M4_STRIPS][256][32], then [2][16][32] rows of B
     u64 *Bt = T + M4_STRIPS * 256 * M4_CTA_WORDS;
     __shared__ __align__(8) u64 bfull[2];
+    constexpr int M4_ROWS_PER_WARP = M4_CTA_ROWS / WARPS;  // 64 or 32
+    constexpr int H = M4_ROWS_PER_WARP / 32;                 // rows per lane held for A
+    constexpr int WALK = 2 * 256 / WARPS;                     // Gray-walk entries per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 row0 = (i64)blockIdx.y * M4_CTA_ROWS + warp * M4_ROWS_PER_WARP;
     const i64 cw = (i64)blockIdx.x * M4_CTA_WORDS + lane;  // this lane's column word
     const i64 ncw = words_of(n), kw = words_of(k);
     const bool col_ok = cw < ncw;
 
-    // table-build role: strip bstrip, Gray-walk positions 64*bq .. 64*bq+63
-    const int bstrip = warp >> 2, bq = warp & 3;
+    // table-build role: strip bstrip, Gray-walk positions WALK*bq .. WALK*bq+WALK-1
+    const int bstrip = warp / (WARPS / 2), bq = warp % (WARPS / 2);
 
     u64 acc[M4_ROWS_PER_WARP];
 #pragma unroll
@@ -96,16 +98,16 @@ gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, 
         ptx::mbar_arrive_expect_tx(&bfull[buf], M4_BTILE_WORDS * 8);
         ptx::tma_load_2d(Bt + buf * M4_BTILE_WORDS, &bmap, &bfull[buf], cw0, (int)(st * 16));
     };
-    // A: word w of K for rows row0 + lane and row0 + 32 + lane
-    auto load_a = [&](i64 w, u64 (&av)[2]) {
+    // A: word w of K for rows row0 + 32h + lane
+    auto load_a = [&](i64 w, u64 (&av)[H]) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < H; ++h) {
             const i64 r = row0 + 32 * h + lane;
             av[h] = (r < m && w < kw) ? __ldg(A + r * lda + w) : 0ull;
         }
     };
 
-    u64 bv[8], av[2], av_next[2];
+    u64 bv[8], av[H], av_next[H];
     if constexpr (kTma) {
         if (threadIdx.x == 0) {
             ptx::prefetch_tmap(&bmap);
@@ -143,23 +145,24 @@ gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, 
         }
         {
             u64 *Ts = T + (size_t)bstrip * 256 * M4_CTA_WORDS + lane;
-            const int i0 = 64 * bq;
+            const int i0 = WALK * bq;
             const int g0 = i0 ^ (i0 >> 1);
             u64 val = 0;
 #pragma unroll
             for (int b = 0; b < 8; ++b)
                 if ((g0 >> b) & 1) val ^= bv[b];
-            gray_walk<0>(Ts, i0, val, bv);
+            gray_walk<0, WALK>(Ts, i0, val, bv);
         }
         __syncthreads();
-        // the 16 bits of K of this stage for rows lane and 32 + lane
-        const u32 ix0 = (u32)(av[0] >> (16 * sub)) & 0xffffu;
-        const u32 ix1 = (u32)(av[1] >> (16 * sub)) & 0xffffu;
+        // the 16 bits of K of this stage for rows 32h + lane
+        u32 ix[H];
+#pragma unroll
+        for (int h = 0; h < H; ++h) ix[h] = (u32)(av[h] >> (16 * sub)) & 0xffffu;
         if (st + 1 < nstages) {
             if constexpr (!kTma) load_b(st + 1, bv);
             if (sub == 3) {
-                av[0] = av_next[0];
-                av[1] = av_next[1];
+#pragma unroll
+                for (int h = 0; h < H; ++h) av[h] = av_next[h];
                 load_a((st + 1) / 4 + 1, av_next);
             }
         }
@@ -167,8 +170,8 @@ gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, 
         const u64 *T1 = T + 256 * M4_CTA_WORDS + lane;
 #pragma unroll
         for (int r = 0; r < M4_ROWS_PER_WARP; ++r) {
-            const u32 ix = __shfl_sync(0xffffffffu, r < 32 ? ix0 : ix1, r & 31);
-            acc[r] ^= T0[(ix & 255u) * M4_CTA_WORDS] ^ T1[(ix >> 8) * M4_CTA_WORDS];
+            const u32 x = __shfl_sync(0xffffffffu, ix[r / 32], r & 31);
+            acc[r] ^= T0[(x & 255u) * M4_CTA_WORDS] ^ T1[(x >> 8) * M4_CTA_WORDS];
         }
     }
 
@@ -182,7 +185,7 @@ gemm_m4ri_kernel(const u64 *__restrict__ A, i64 lda, const u64 *__restrict__ B, 
 }
 
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc, i64 m,
-                             i64 k, i64 n, cudaStream_t s)
+                             i64 k, i64 n, cudaStream_t s, int tile)
 {
     if (m <= 0 || n <= 0) return MELA_OK;
     if (k <= 0) {
@@ -204,16 +207,18 @@ mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *
                      make_u64_rows_map(&bmap, B, k, words_of(n), ldb, M4_CTA_WORDS, 16) == MELA_OK;
     u32 *err = device_error_word();
     const dim3 grid((unsigned)gx, (unsigned)gy);
-    if (tma) {
-        MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_m4ri_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           smem));
-        gemm_m4ri_kernel<true><<<grid, 256, smem, s>>>(A, lda, B, ldb, C, ldc, m, k, n, bmap, err);
-    } else {
-        cudaGetLastError();
-        MELA_CUDA_TRY(cudaFuncSetAttribute(gemm_m4ri_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           smem));
-        gemm_m4ri_kernel<false><<<grid, 256, smem, s>>>(A, lda, B, ldb, C, ldc, m, k, n, bmap, err);
-    }
+    if (!tma) cudaGetLastError();
+    auto launch = [&](auto kernel, int threads) -> mela_status {
+        MELA_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kernel<<<grid, threads, smem, s>>>(A, lda, B, ldb, C, ldc, m, k, n, bmap, err);
+        return MELA_OK;
+    };
+    mela_status st;
+    if (tile == 1)
+        st = tma ? launch(gemm_m4ri_kernel<8, true>, 256) : launch(gemm_m4ri_kernel<8, false>, 256);
+    else
+        st = tma ? launch(gemm_m4ri_kernel<16, true>, 512) : launch(gemm_m4ri_kernel<16, false>, 512);
+    if (st != MELA_OK) return st;
     MELA_LAUNCH_CHECK("gemm_m4ri_kernel");
     return MELA_OK;
 }

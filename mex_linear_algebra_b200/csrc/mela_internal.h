@@ -52,8 +52,9 @@ mela_status make_u8_kmajor_map(CUtensorMap *map, const unsigned char *base, i64 
 // no swizzle, zeros read past the edges.
 mela_status make_u64_rows_map(CUtensorMap *map, const u64 *base, i64 rows, i64 words, i64 ld, int box_words,
                               int box_rows);
+// tile: 0 / 2 = 16 warps of 32 rows per 512-row CTA, 1 = 8 warps of 64 rows.
 mela_status launch_gemm_m4ri(const u64 *A, i64 lda, const u64 *B, i64 ldb, u64 *C, i64 ldc,
-                             i64 m, i64 k, i64 n, cudaStream_t s);
+                             i64 m, i64 k, i64 n, cudaStream_t s, int tile = 0);
 
 // Whole RREF of one matrix in one single-CTA launch (batch.cu).
 size_t fused_workspace(i64 m, i64 n);

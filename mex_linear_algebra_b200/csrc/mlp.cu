@@ -15,6 +15,7 @@
 // parameter and block), Adam update (one thread per parameter).
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 
 #include "mela_common.cuh"
@@ -161,36 +162,58 @@ __global__ void adam_kernel(float *__restrict__ params, const float *__restrict_
 // build) is installed when the library loads; mela_costmodel_load replaces
 // or removes it.
 #include "costmodel_weights.inc"
+// Installed weights: an immutable snapshot swapped under the mutex and read
+// through a shared pointer, so an evaluation neither copies the weights nor
+// holds the lock while it runs.
+struct CostModelWeights {
+    float p[kParams];
+};
 static std::mutex g_cm_mu;
-static float g_cm[kParams];
-static bool g_cm_loaded = false;
+static std::shared_ptr<const CostModelWeights> g_cm;
+
+static std::shared_ptr<const CostModelWeights> current_model()
+{
+    std::lock_guard<std::mutex> g(g_cm_mu);
+    return g_cm;
+}
+
 #ifdef MELA_DEFAULT_MODEL
 static_assert(sizeof kDefaultModel / sizeof kDefaultModel[0] == kParams, "compiled-in model size");
 static const bool g_cm_default = [] {
-    std::memcpy(g_cm, kDefaultModel, sizeof g_cm);
-    g_cm_loaded = true;
+    auto w = std::make_shared<CostModelWeights>();
+    std::memcpy(w->p, kDefaultModel, sizeof w->p);
+    g_cm = w;
     return true;
 }();
 #endif
 
+// The network on the host, layer by layer along contiguous weight rows.
 static void host_forward(const float *P, const float *x, float *y)
 {
-    float h1[kH1], h2[kH2];
+    float h1[kH1], h2[kH2], o[kOut];
+    for (int j = 0; j < kH1; ++j) h1[j] = P[ob1 + j];
+    for (int i = 0; i < kIn; ++i) {
+        const float xi = x[i];
+        const float *w = P + oW1 + i * kH1;
+        for (int j = 0; j < kH1; ++j) h1[j] += xi * w[j];
+    }
+    for (int j = 0; j < kH1; ++j) h1[j] = h1[j] > 0.f ? h1[j] : 0.f;
+    for (int k = 0; k < kH2; ++k) h2[k] = P[ob2 + k];
     for (int j = 0; j < kH1; ++j) {
-        float a = P[ob1 + j];
-        for (int i = 0; i < kIn; ++i) a += x[i] * P[oW1 + i * kH1 + j];
-        h1[j] = a > 0.f ? a : 0.f;
+        const float hj = h1[j];
+        if (hj == 0.f) continue;
+        const float *w = P + oW2 + j * kH2;
+        for (int k = 0; k < kH2; ++k) h2[k] += hj * w[k];
     }
+    for (int k = 0; k < kH2; ++k) h2[k] = h2[k] > 0.f ? h2[k] : 0.f;
+    for (int q = 0; q < kOut; ++q) o[q] = P[ob3 + q];
     for (int k = 0; k < kH2; ++k) {
-        float a = P[ob2 + k];
-        for (int j = 0; j < kH1; ++j) a += h1[j] * P[oW2 + j * kH2 + k];
-        h2[k] = a > 0.f ? a : 0.f;
+        const float hk = h2[k];
+        if (hk == 0.f) continue;
+        const float *w = P + oW3 + k * kOut;
+        for (int q = 0; q < kOut; ++q) o[q] += hk * w[q];
     }
-    for (int o = 0; o < kOut; ++o) {
-        float a = P[ob3 + o];
-        for (int k = 0; k < kH2; ++k) a += h2[k] * P[oW3 + k * kOut + o];
-        y[o] = a;
-    }
+    for (int q = 0; q < kOut; ++q) y[q] = o[q];
 }
 
 void costmodel_features(int op, double m, double n, double p, double density, double batch_count,
@@ -211,24 +234,16 @@ void costmodel_features(int op, double m, double n, double p, double density, do
     x[9] = (float)(batch_log2_cells / 28.0);
 }
 
-bool costmodel_loaded()
-{
-    std::lock_guard<std::mutex> g(g_cm_mu);
-    return g_cm_loaded;
-}
+bool costmodel_loaded() { return current_model() != nullptr; }
 
 bool costmodel_predict(int op, double m, double n, double p, double density, double batch_count,
                        double batch_log2_cells, float *y_out)
 {
-    float P[kParams];
-    {
-        std::lock_guard<std::mutex> g(g_cm_mu);
-        if (!g_cm_loaded) return false;
-        std::memcpy(P, g_cm, sizeof P);
-    }
+    const std::shared_ptr<const CostModelWeights> w = current_model();
+    if (!w) return false;
     float x[kIn], y[kOut];
     costmodel_features(op, m, n, p, density, batch_count, batch_log2_cells, x);
-    host_forward(P, x, y);
+    host_forward(w->p, x, y);
     const int nc = config_count(op);
     for (int o = 0; o < nc; ++o) y_out[o] = y[o];
     return true;
@@ -299,13 +314,13 @@ extern "C" mela_status mela_mlp_adam_step(float *d_params, const float *d_grad, 
 
 extern "C" mela_status mela_costmodel_load(const float *h_params)
 {
-    std::lock_guard<std::mutex> g(g_cm_mu);
-    if (!h_params) {
-        g_cm_loaded = false;
-        return MELA_OK;
+    std::shared_ptr<CostModelWeights> w;
+    if (h_params) {
+        w = std::make_shared<CostModelWeights>();
+        std::memcpy(w->p, h_params, sizeof w->p);
     }
-    std::memcpy(g_cm, h_params, sizeof g_cm);
-    g_cm_loaded = true;
+    std::lock_guard<std::mutex> g(g_cm_mu);
+    g_cm = std::move(w);
     return MELA_OK;
 }
 

@@ -53,3 +53,21 @@ def test_rank_and_null_blocked_upload(cuda, shape, kind):
     if m * n <= 40_000_000:
         Z = mela.mela_null_gf2(H)
         assert np.array_equal(Z, O.null_logical(_bits(H)))
+
+
+def test_large_arrays_take_the_blocked_upload(cuda):
+    """A 32 MiB double array goes through the page-locked staging slots in
+    column blocks (mela_upload_stats_get), a 1 MiB one is copied directly."""
+    import ctypes as C
+    from mex_linear_algebra_b200 import _lib, mela
+    L = _lib.lib()
+    st = _lib.UploadStats()
+    L.mela_upload_stats_get(C.byref(st), 1)
+    A = _double(5, 2048, 2048)            # 32 MiB
+    B = _double(6, 2048, 64)              # 1 MiB
+    C_ = mela.mela_matmul_gf2(A, B)
+    L.mela_upload_stats_get(C.byref(st), 1)
+    assert st.blocked_bytes == A.nbytes and st.blocks >= 4
+    assert st.direct_bytes == B.nbytes
+    want = O.unpack(O.matmul(O.pack(A), O.pack(B), 2048, 2048, 64), 2048, 64)
+    assert np.array_equal(C_, want)

@@ -56,14 +56,15 @@ def test_configurations_match_the_library():
         tune(_lib.ELIM_M4RI, 10, 3), _lib.ELIM_FUSED, _lib.ELIM_TC)
     assert costmodel.config_codes("null") == costmodel.config_codes("rank")
     assert costmodel.config_codes("matmul") == (
-        _lib.GEMM_PLAIN, _lib.GEMM_M4RI, tune(_lib.GEMM_TC, 0, 2), tune(_lib.GEMM_TC, 0, 1),
-        tune(_lib.GEMM_TC_FP4, 0, 2), tune(_lib.GEMM_TC_FP4, 0, 1))
+        _lib.GEMM_PLAIN, _lib.GEMM_M4RI, tune(_lib.GEMM_M4RI, 0, 1), tune(_lib.GEMM_TC, 0, 2),
+        tune(_lib.GEMM_TC, 0, 1), tune(_lib.GEMM_TC_FP4, 0, 2), tune(_lib.GEMM_TC_FP4, 0, 1))
     assert costmodel.config_codes("batch") == (0, 1, 2)
     for op in ("rank", "matmul", "batch"):
         assert len(costmodel.CONFIG_NAMES[op]) == L.mela_costmodel_config_count(costmodel.OPS[op])
         assert L.mela_costmodel_config(costmodel.OPS[op], len(costmodel.CONFIG_NAMES[op])) == -1
     for v in costmodel.config_codes("matmul"):
-        assert L.mela_matmul_workspace_size(v, 2048, 2048, 2048) > 0 or v == _lib.GEMM_M4RI
+        # the Four-Russians product needs no workspace; every other form does
+        assert (L.mela_matmul_workspace_size(v, 2048, 2048, 2048) > 0) == (_lib.GEMM_M4RI != (v & 0xff))
 
 
 def test_bad_tuning_fields_are_rejected_before_device_work():
@@ -79,7 +80,8 @@ def test_bad_tuning_fields_are_rejected_before_device_work():
     for v in bad_elim:
         for fn in (L.mela_dev_rank, L.mela_dev_rref):
             assert fn(v, fake, 2, 100, 100, fake, fake, fake, fake, 1 << 20, None) == _lib.ERR_INVALID, hex(v)
-    bad_gemm = [tune(_lib.GEMM_TC, 0, 3), tune(_lib.GEMM_M4RI, 6), tune(_lib.GEMM_PLAIN, 0, 1), 5]
+    bad_gemm = [tune(_lib.GEMM_TC, 0, 3), tune(_lib.GEMM_M4RI, 6), tune(_lib.GEMM_M4RI, 0, 3),
+                tune(_lib.GEMM_PLAIN, 0, 1), 5]
     for v in bad_gemm:
         assert L.mela_dev_matmul(v, fake, 2, fake, 2, fake, 2, 100, 100, 100, fake, 1 << 30, None) \
             == _lib.ERR_INVALID, hex(v)
