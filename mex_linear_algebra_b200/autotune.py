@@ -181,15 +181,38 @@ def time_request(req, reps=3, extra=None):
     return out
 
 
+def stratified(reqs, count: int, bins: int = 12):
+    """About `count` requests of `reqs`, an equal share from each of `bins`
+    log2-size bins (bits touched: m*n, plus n*p for products), evenly spaced
+    within each bin."""
+    cells = np.array([r["m"] * r["n"] + (r["n"] * r["p"] if r["op"] == "matmul" else 0) for r in reqs],
+                     dtype=np.float64)
+    lg = np.log2(cells)
+    edges = np.linspace(lg.min(), lg.max() + 1e-9, bins + 1)
+    per = max(1, count // bins)
+    out = []
+    for b in range(bins):
+        idx = np.nonzero((lg >= edges[b]) & (lg < edges[b + 1]))[0]
+        if len(idx):
+            out.extend(int(i) for i in np.unique(idx[np.linspace(0, len(idx) - 1, min(per, len(idx))).astype(np.int64)]))
+    return [reqs[i] for i in sorted(out)]
+
+
 def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 7e7, batch_count: int = 0,
-             verbose: bool = False, out: str | None = None, budget_s: float = 0.0):
+             verbose: bool = False, out: str | None = None, budget_s: float = 0.0, window: int = 0):
     """Time `count` requests of the mixed stream from request `offset` on
     (requests above `max_cells` bits are skipped; the stream's largest,
     8192 x 8192, is 6.7e7), then `batch_count` batch requests.  With `out`
     the records so far are written there every 25 requests; with `budget_s`
     each part stops once it has used its share of that many seconds."""
     import torch
-    reqs = gen.mixed_stream(offset + count, SEED)[offset:]
+    if window > count:
+        # `count` requests spread evenly over log2-size bins of a window of
+        # `window` requests: the large requests, which dominate total time,
+        # get as many records as the small ones
+        reqs = stratified(gen.mixed_stream(offset + window, SEED)[offset:], count)
+    else:
+        reqs = gen.mixed_stream(offset + count, SEED)[offset:]
     db = []
     t0 = time.time()
 
@@ -207,7 +230,7 @@ def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 7e7, bat
         if (i + 1) % 25 == 0:
             save()
             if verbose:
-                print(f"{i + 1}/{count} timed, {time.time() - t0:.1f}s", flush=True)
+                print(f"{i + 1}/{len(reqs)} timed, {time.time() - t0:.1f}s", flush=True)
         if budget_s and time.time() - t0 > share:
             break
     t1 = time.time()
@@ -231,10 +254,12 @@ def main():
     ap.add_argument("--batches", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--budget", type=float, default=0.0, help="seconds (0: no limit)")
+    ap.add_argument("--window", type=int, default=0,
+                    help="pick --count requests stratified by size from this many (0: consecutive)")
     ap.add_argument("--out", default="autotune_db.json")
     a = ap.parse_args()
     db = build_db(a.count, a.offset, a.reps, batch_count=a.batches, verbose=True, out=a.out,
-                  budget_s=a.budget)
+                  budget_s=a.budget, window=a.window)
     print(f"{len(db)} records -> {a.out}; all configurations agree: {all(r['agree'] for r in db)}")
 
 
