@@ -600,13 +600,21 @@ def bench_dispatch(torch, per_bin=14, bins=8):
     from mex_linear_algebra_b200._lib import lib
     if lib().mela_costmodel_choose(_lib.OP_RANK, 100, 100, 0, 0.5, 1, 13.3) < 0:
         return {"unavailable": "the library was built without a trained cost model"}
+    import ctypes as C
     sample = _stratified(gen.mixed_stream(50000, 4), per_bin, bins)
     recs = []
     t0 = time.time()
+    codes = {op: dict(zip(costmodel.config_codes(op), costmodel.CONFIG_NAMES[op])) for op in ("rank", "null", "matmul")}
+    measured = 0
     for r in sample:
-        recs.append(autotune.time_request(r, reps=2, extra={"auto": 0}))
+        rec = autotune.time_request(r, reps=2, extra={"auto": 0})
+        # the configuration the last AUTO call (the timed ones above) resolved to
+        d = C.c_double(0)
+        rec["auto_choice"] = codes[r["op"]].get(int(lib().mela_dispatch_last(C.byref(d))))
+        measured += int(d.value >= 0)
+        recs.append(rec)
         torch.cuda.empty_cache()
-    tot = {"best": 0.0, "auto": 0.0, "rule": 0.0}
+    tot = {"best": 0.0, "auto": 0.0, "rule": 0.0, "auto_choice": 0.0}
     per = {"auto": [], "rule": []}
     by_op = {}
     for r in recs:
@@ -616,6 +624,7 @@ def bench_dispatch(torch, per_bin=14, bins=8):
         tot["best"] += best
         tot["auto"] += t["auto"]
         tot["rule"] += rule
+        tot["auto_choice"] += t.get(r["auto_choice"], t["auto"])
         per["auto"].append(t["auto"] / best - 1)
         per["rule"].append(rule / best - 1)
         o = by_op.setdefault(r["op"], {"requests": 0, "best_us": 0.0, "auto_us": 0.0, "rule_us": 0.0})
@@ -633,6 +642,8 @@ def bench_dispatch(torch, per_bin=14, bins=8):
                       "bins from the smallest to the 8192 x 8192 ones; every configuration timed "
                       "(median of 2 after a warm-up)",
             "library_auto_regret": round(tot["auto"] / tot["best"] - 1, 4),
+            "auto_choice_regret": round(tot["auto_choice"] / tot["best"] - 1, 4),
+            "density_measured": f"{measured} of {len(recs)} AUTO calls read the density back",
             "fixed_rule_regret": round(tot["rule"] / tot["best"] - 1, 4),
             "auto_speedup_vs_rule": round(tot["rule"] / tot["auto"], 4),
             "mean_request_regret": {"auto": round(float(np.mean(per["auto"])), 4),
@@ -642,8 +653,10 @@ def bench_dispatch(torch, per_bin=14, bins=8):
             "all_configurations_bit_identical": all(r["agree"] for r in recs),
             "seconds": round(time.time() - t0, 1),
             "note": "auto = mela_dev_rank / mela_dev_rref (+ null basis) / mela_dev_matmul with the AUTO "
-                    "variant: one popcount of the input and an 8-byte read-back, the model on the host, "
-                    "then the chosen configuration"}
+                    "variant timed as a whole: the model on the host at four densities, a popcount of the "
+                    "input and an 8-byte read-back when the choice depends on the density, then the "
+                    "chosen configuration; auto_choice = the recorded time of the configuration AUTO "
+                    "chose (the choice without the call's own overhead)"}
 
 
 def run_mela(args, ws, rank, local):

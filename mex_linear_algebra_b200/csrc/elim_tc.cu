@@ -949,6 +949,7 @@ constexpr size_t kMaxElimSeen = 64;
 std::mutex g_elim_graph_mu;
 std::vector<ElimGraph> *g_elim_graphs = nullptr;
 std::vector<ElimGraphKey> *g_elim_seen = nullptr;  // calls made once, without a graph
+size_t g_elim_seen_next = 0;                       // the oldest entry, replaced once the list is full
 
 bool elim_graphs_enabled()
 {
@@ -980,7 +981,14 @@ bool elim_graph_capturable(const ElimGraphKey &k, cudaStream_t s)
     if (!g_elim_seen) g_elim_seen = new std::vector<ElimGraphKey>();
     for (const ElimGraphKey &q : *g_elim_seen)
         if (std::memcmp(&q, &k, sizeof k) == 0) return true;
-    if (g_elim_seen->size() < kMaxElimSeen) g_elim_seen->push_back(k);
+    // remember the call; a full list forgets its oldest entry, so a stream of
+    // one-off shapes never keeps a repeated call from being captured
+    if (g_elim_seen->size() < kMaxElimSeen) {
+        g_elim_seen->push_back(k);
+    } else {
+        (*g_elim_seen)[g_elim_seen_next] = k;
+        g_elim_seen_next = (g_elim_seen_next + 1) % kMaxElimSeen;
+    }
     return false;
 }
 void elim_graph_store(const ElimGraphKey &k, cudaGraphExec_t exec)
