@@ -430,10 +430,16 @@ int32_t mela_costmodel_choose(int32_t op, int64_t m, int64_t n, int64_t p, doubl
  * that count, or -1 when no model is installed. */
 int32_t mela_costmodel_predict(int32_t op, int64_t m, int64_t n, int64_t p, double density,
                                int64_t batch_count, double batch_log2_cells, float *y);
+/* What an AUTO call decides before it sees the data (ops rank, null space,
+ * product): the configuration index whose worst predicted loss over
+ * densities 0.001, 0.01, 0.1 and 0.5 is smallest, and in *measure whether
+ * that loss exceeds the cost of measuring the density (about 15 us), in
+ * which case the call counts the input's ones and asks the model again.
+ * -1 without a model. */
+int32_t mela_costmodel_plan(int32_t op, int64_t m, int64_t n, int64_t p, int32_t *measure);
 /* The variant argument the calling thread's last AUTO call resolved to (-1
  * before any), and in *density the density it measured on the device for
- * the choice, or a negative value when none was needed: the density is read
- * back only when the model's choice differs across densities 0.001 .. 0.5. */
+ * the choice, or a negative value when none was needed (mela_costmodel_plan). */
 int32_t mela_dispatch_last(double *density);
 /* The MELA_MLP_IN input features of a request. */
 void mela_costmodel_features(int32_t op, int64_t m, int64_t n, int64_t p, double density,

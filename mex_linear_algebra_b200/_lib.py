@@ -119,6 +119,7 @@ SIGNATURES = {
     "mela_costmodel_features": (None, [_i32, _i64, _i64, _i64, C.c_double, _i64, C.c_double, _vp]),
     "mela_costmodel_config_count": (_i32, [_i32]),
     "mela_dispatch_last": (_i32, [C.POINTER(C.c_double)]),
+    "mela_costmodel_plan": (_i32, [_i32, _i64, _i64, _i64, C.POINTER(_i32)]),
     "mela_costmodel_predict": (_i32, [_i32, _i64, _i64, _i64, C.c_double, _i64, C.c_double, _vp]),
     "mela_costmodel_config": (_i32, [_i32, _i32]),
     "mela_dev_popcount": (_st, [_vp, _i64, _i64, _i64, _vp, _vp]),

@@ -220,17 +220,18 @@ static int32_t remember(int32_t v, double density)
 // smallest) is taken as it is.
 constexpr double kMeasureCostUs = 15.0;
 
-static int choose_measuring(int op, double m, double n, double p, double cells,
-                            const u64 *M, i64 ld, i64 rows, i64 cols, cudaStream_t s)
+// Without the density: the configuration whose worst predicted loss over
+// the probed densities is smallest (index), and whether that loss exceeds
+// what measuring costs.  -1 without a model.
+static int choose_unmeasured(int op, double m, double n, double p, double cells, bool *measure)
 {
-    static const double probe[] = {0.001, 0.01, 0.1, 0.5};
-    constexpr int kProbes = 4;
+    static const double probe[kCostProbes] = {0.001, 0.01, 0.1, 0.5};
     const double lc = std::log2(cells > 1 ? cells : 1);
     const int nc = config_count(op);
-    float y[kProbes][MELA_MLP_OUT];
-    double best[kProbes];
-    for (int d = 0; d < kProbes; ++d) {
-        if (!costmodel_predict(op, m, n, p, probe[d], 1, lc, y[d])) return -1;
+    float y[kCostProbes][MELA_MLP_OUT];
+    double best[kCostProbes];
+    if (nc <= 0 || !costmodel_predict_densities(op, m, n, p, probe, 1, lc, y)) return -1;
+    for (int d = 0; d < kCostProbes; ++d) {
         best[d] = 1e300;
         for (int c = 0; c < nc; ++c) best[d] = std::fmin(best[d], std::exp2((double)y[d][c]));
     }
@@ -238,17 +239,26 @@ static int choose_measuring(int op, double m, double n, double p, double cells,
     double pick_loss = 1e300;
     for (int c = 0; c < nc; ++c) {
         double loss = 0;
-        for (int d = 0; d < kProbes; ++d) loss = std::fmax(loss, std::exp2((double)y[d][c]) - best[d]);
+        for (int d = 0; d < kCostProbes; ++d) loss = std::fmax(loss, std::exp2((double)y[d][c]) - best[d]);
         if (loss < pick_loss) {
             pick_loss = loss;
             pick = c;
         }
     }
+    *measure = pick_loss > kMeasureCostUs;
+    return pick;
+}
+
+static int choose_measuring(int op, double m, double n, double p, double cells,
+                            const u64 *M, i64 ld, i64 rows, i64 cols, cudaStream_t s)
+{
+    bool measure = false;
+    const int pick = choose_unmeasured(op, m, n, p, cells, &measure);
     t_last_density = -1.0;
-    if (pick_loss <= kMeasureCostUs) return pick;
+    if (pick < 0 || !measure) return pick;
     const double d = measure_density(M, ld, rows, cols, s);
     t_last_density = d;
-    return costmodel_choose(op, m, n, p, d, 1, lc);
+    return costmodel_choose(op, m, n, p, d, 1, std::log2(cells > 1 ? cells : 1));
 }
 
 // ---------------------------------------------------------------- choices
@@ -300,6 +310,16 @@ int32_t fixed_elim_variant(i64 m, i64 n)
 using namespace mela;
 
 extern "C" int32_t mela_costmodel_config_count(int32_t op) { return config_count(op); }
+
+extern "C" int32_t mela_costmodel_plan(int32_t op, int64_t m, int64_t n, int64_t p, int32_t *measure)
+{
+    if (op != MELA_OP_RANK && op != MELA_OP_NULL && op != MELA_OP_MATMUL) return -1;
+    bool ms = false;
+    // products: m x n times n x p, the density is A's (m x n)
+    const int c = choose_unmeasured(op, (double)m, (double)n, (double)p, (double)m * (double)n, &ms);
+    if (measure) *measure = ms ? 1 : 0;
+    return c;
+}
 
 extern "C" int32_t mela_dispatch_last(double *density)
 {

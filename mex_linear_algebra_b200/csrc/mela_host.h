@@ -71,6 +71,10 @@ bool costmodel_predict(int op, double m, double n, double p, double density, dou
                        double batch_log2_cells, float *y);
 void costmodel_features(int op, double m, double n, double p, double density, double batch_count,
                         double batch_log2_cells, float *x);
+// The predictions at kCostProbes densities dens[] at once; false without a model.
+constexpr int kCostProbes = 4;
+bool costmodel_predict_densities(int op, double m, double n, double p, const double *dens, double batch_count,
+                                 double batch_log2_cells, float (*y)[MELA_MLP_OUT]);
 size_t gemm_workspace(int variant, i64 m, i64 k, i64 n);
 mela_status gemm_prepare(int variant, const u64 *A, i64 lda, const u64 *B, i64 ldb, i64 m, i64 k,
                          i64 n, void *ws, size_t ws_bytes, cudaStream_t s);

@@ -249,6 +249,59 @@ bool costmodel_predict(int op, double m, double n, double p, double density, dou
     return true;
 }
 
+// Predictions for one request at kProbe densities in one pass: the inputs
+// differ only in the density feature, so the first layer is shared and the
+// other two run with the probes side by side (the inner loops over the four
+// probes vectorise).
+bool costmodel_predict_densities(int op, double m, double n, double p, const double *dens, double batch_count,
+                                 double batch_log2_cells, float (*y_out)[MELA_MLP_OUT])
+{
+    constexpr int NP = kCostProbes;
+    const std::shared_ptr<const CostModelWeights> w = current_model();
+    if (!w) return false;
+    const float *P = w->p;
+    float x[kIn];
+    costmodel_features(op, m, n, p, 0.5, batch_count, batch_log2_cells, x);
+    float base[kH1];
+    for (int j = 0; j < kH1; ++j) base[j] = P[ob1 + j];
+    for (int i = 0; i < kIn; ++i) {
+        if (i == 3) continue;  // the density feature, added per probe below
+        const float xi = x[i];
+        const float *wr = P + oW1 + i * kH1;
+        for (int j = 0; j < kH1; ++j) base[j] += xi * wr[j];
+    }
+    float xd[NP];
+    for (int q = 0; q < NP; ++q) {
+        const double d = dens[q] > 1e-6 ? dens[q] : 1e-6;
+        xd[q] = (float)(std::log10(d) / 3.0 + 1.0);
+    }
+    float h1[kH1][NP], h2[kH2][NP], o[kOut][NP];
+    for (int j = 0; j < kH1; ++j)
+        for (int q = 0; q < NP; ++q) {
+            const float a = base[j] + xd[q] * P[oW1 + 3 * kH1 + j];
+            h1[j][q] = a > 0.f ? a : 0.f;
+        }
+    for (int k = 0; k < kH2; ++k)
+        for (int q = 0; q < NP; ++q) h2[k][q] = P[ob2 + k];
+    for (int j = 0; j < kH1; ++j) {
+        const float *wr = P + oW2 + j * kH2;
+        for (int k = 0; k < kH2; ++k)
+            for (int q = 0; q < NP; ++q) h2[k][q] += h1[j][q] * wr[k];
+    }
+    for (int k = 0; k < kH2; ++k)
+        for (int q = 0; q < NP; ++q) h2[k][q] = h2[k][q] > 0.f ? h2[k][q] : 0.f;
+    for (int c = 0; c < kOut; ++c)
+        for (int q = 0; q < NP; ++q) o[c][q] = P[ob3 + c];
+    for (int k = 0; k < kH2; ++k) {
+        const float *wr = P + oW3 + k * kOut;
+        for (int c = 0; c < kOut; ++c)
+            for (int q = 0; q < NP; ++q) o[c][q] += h2[k][q] * wr[c];
+    }
+    for (int q = 0; q < NP; ++q)
+        for (int c = 0; c < kOut; ++c) y_out[q][c] = o[c][q];
+    return true;
+}
+
 // -1 when no model is loaded (callers use their fixed rule)
 int costmodel_choose(int op, double m, double n, double p, double density, double batch_count,
                      double batch_log2_cells)

@@ -170,3 +170,29 @@ def test_trained_model_beats_fixed_rule():
     assert tot_model / tot_best - 1 < tot_rule / tot_best - 1
     # per request, too: the mean slowdown against the exhaustive best shrinks
     assert np.mean(per_model) < np.mean(per_rule)
+
+
+def test_dispatch_plan_before_the_data():
+    """What AUTO decides before seeing the data, recomputed from the model's
+    own predictions at the four probe densities: the configuration with the
+    smallest worst-case predicted loss, and a density read-back only when
+    that loss exceeds 15 microseconds.  Host-side, no GPU."""
+    import ctypes as C
+    from mex_linear_algebra_b200 import _lib, costmodel, gen
+    L = _lib.lib()
+    costmodel.install_default()
+    if L.mela_costmodel_choose(_lib.OP_RANK, 100, 100, 0, 0.5, 1, 13.3) < 0:
+        pytest.skip("the library was built without a trained model")
+    probes = (0.001, 0.01, 0.1, 0.5)
+    for r in gen.mixed_stream(400, 4)[::7]:
+        op, m, n, p = r["op"], r["m"], r["n"], r.get("p", 0)
+        ys = [costmodel.predict_host(op, m, n, p, d) for d in probes]
+        names = costmodel.CONFIG_NAMES[op]
+        best = [min(2.0 ** v for v in y.values()) for y in ys]
+        loss = {c: max(2.0 ** y[c] - b for y, b in zip(ys, best)) for c in names}
+        want = min(names, key=lambda c: loss[c])
+        meas = C.c_int32(-1)
+        got = L.mela_costmodel_plan(costmodel.OPS[op], m, n, p, C.byref(meas))
+        assert names[got] == want or abs(loss[names[got]] - loss[want]) < 1e-3 * max(1.0, loss[want]), (r, want)
+        assert meas.value == int(loss[names[got]] > 15.0)
+
