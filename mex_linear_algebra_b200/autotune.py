@@ -13,8 +13,9 @@ is the judge of the model's regret.
 
 Requests: the mixed stream of rank, null-space and product requests (m, n,
 p log-uniform in [32, 8192], density log-uniform in [0.001, 0.5],
-``gen.mixed_stream``) and batch requests (``gen.batch_requests``: a batch of
-`count` m x n Bernoulli matrices; per-matrix time of each engine).
+``gen.mixed_stream``) and batch requests, half broad (``gen.batch_requests``)
+and half shaped like parity-check batches (``gen.batch_requests_sparse``):
+a batch of `count` m x n Bernoulli matrices; per-matrix time of each engine.
 
     python -m mex_linear_algebra_b200.autotune --count 600 --offset 100000 --out db.json
 """
@@ -234,7 +235,9 @@ def build_db(count: int, offset: int, reps: int = 3, max_cells: float = 7e7, bat
         if budget_s and time.time() - t0 > share:
             break
     t1 = time.time()
-    for j, r in enumerate(gen.batch_requests(batch_count, SEED, offset)):
+    breqs = gen.batch_requests(batch_count - batch_count // 2, SEED, offset) + \
+        gen.batch_requests_sparse(batch_count // 2, SEED, offset)
+    for j, r in enumerate(breqs):
         db.append(time_request(r, reps))
         torch.cuda.empty_cache()
         if (j + 1) % 25 == 0:

@@ -182,6 +182,29 @@ def batch_requests(count: int, seed: int = 4, offset: int = 0):
     return out
 
 
+def batch_requests_sparse(count: int, seed: int = 4, offset: int = 0):
+    """Batch requests shaped like parity-check batches: m log-uniform in
+    [48, 600], n = m * [1.5, 2.5], density log-uniform in [0.003, 0.1],
+    1024, 4096 or 16384 matrices (fewer when the batch would pass 2^31
+    bits).  Word layout per request r: 4 words of stream 2 at 4(offset + r)."""
+    if count <= 0:
+        return []
+    w = words(seed, 2, 4 * offset, 4 * count).reshape(count, 4).astype(np.float64) / 2.0 ** 64
+    m = np.exp(np.log(48.0) + (np.log(600.0) - np.log(48.0)) * w[:, 0])
+    n = m * (1.5 + w[:, 1])
+    dens = np.exp(np.log(0.003) + (np.log(0.1) - np.log(0.003)) * w[:, 2])
+    cnt = (1024 * 4 ** np.floor(w[:, 3] * 3)).astype(np.int64)  # 1024, 4096, 16384
+    out = []
+    for i in range(count):
+        mi, ni = int(round(m[i])), int(round(n[i]))
+        c = int(cnt[i])
+        while c > 1024 and c * mi * ni > (1 << 31):
+            c //= 4
+        out.append(dict(op="batch", m=mi, n=ni, p=0, density=float(dens[i]), batch_count=c,
+                        stream=200000 + offset + i))
+    return out
+
+
 def sparse_packed(seed: int, stream: int, m: int, n: int, density: float) -> np.ndarray:
     """Bernoulli(density) packed matrix: bit set when the 16-bit slice of a
     stream word is below density*65536 (4 entries per word)."""
