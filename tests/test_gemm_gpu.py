@@ -242,3 +242,26 @@ def test_tensor_core_forms_odd_shapes(cuda, shape):
     for variant in ("tc", "tc_fp4"):
         got = to_host(D.matmul(to_dev(A), to_dev(B), m, k, n, variant=variant))
         assert np.array_equal(valid_words(got, n), valid_words(want, n)), variant
+
+
+@pytest.mark.parametrize("tile", [1, 2])
+@pytest.mark.parametrize("pad", [0, 1])
+@pytest.mark.parametrize("shape", [(37, 23, 31), (129, 65, 257), (513, 1000, 2049), (1000, 777, 1500),
+                                   (600, 4100, 4096)])
+def test_m4ri_tiles_and_row_pitches(cuda, tile, pad, shape):
+    """The Four-Russians product on 16 warps of 32 rows (tile 2, the default)
+    and 8 warps of 64 rows (tile 1), with B's rows staged by TMA (row pitch a
+    multiple of 16 bytes) or read with plain loads (odd pitch: pad changes
+    which), against the oracle."""
+    import torch
+    from mex_linear_algebra_b200 import _lib
+    D = _dev()
+    m, k, n = shape
+    A = O.rand_dense(17, m, m, k)
+    B = O.rand_dense(17, n, k, n)
+    wn = (n + 63) // 64
+    ldb = wn + pad
+    Bp = np.zeros((k, ldb), dtype=np.uint64)
+    Bp[:, :wn] = B
+    got = to_host(D.matmul(to_dev(A), to_dev(Bp), m, k, n, variant=_lib.tune(_lib.GEMM_M4RI, 0, tile)))
+    assert np.array_equal(valid_words(got, n), O.matmul(A, B, m, k, n))
