@@ -406,8 +406,9 @@ private:
     size_t job_bytes_ = 0;
 };
 
-// Page-locked staging slots of the calling thread, reused across calls: a
-// slot is refilled once the upload that read it has completed.
+// Page-locked staging slots of the calling thread (per device), reused
+// across calls: a slot is refilled once the upload that read it has
+// completed.
 constexpr int kStageSlots = 3;
 constexpr size_t kStageBytes = (size_t)8 << 20;
 struct Staging {
@@ -417,7 +418,8 @@ struct Staging {
     bool ready = false;
     bool failed = false;
 };
-thread_local Staging t_stage;
+// one set per device: events belong to the device they were created on
+thread_local Staging t_stage[kMaxDevices];
 thread_local mela_upload_stats t_upload_stats;
 
 double now_us()
@@ -427,11 +429,11 @@ double now_us()
 
 bool staging_ready()
 {
-    Staging &S = t_stage;
+    Staging &S = t_stage[current_device()];
     if (S.ready) return true;
     if (S.failed) return false;
     for (int i = 0; i < kStageSlots; ++i) {
-        if (cudaMallocHost(&S.slot[i], kStageBytes) != cudaSuccess ||
+        if (cudaHostAlloc(&S.slot[i], kStageBytes, cudaHostAllocPortable) != cudaSuccess ||
             cudaEventCreateWithFlags(&S.read[i], cudaEventDisableTiming) != cudaSuccess) {
             cudaGetLastError();
             S.failed = true;
@@ -461,7 +463,7 @@ static mela_status upload_and_pack_blocks(const mela_host_matrix *M, u64 *dP, i6
     if (st != MELA_OK) return st;
     cudaStream_t sin = nullptr, sout = nullptr;
     if ((st = copy_streams(&sin, &sout)) != MELA_OK) return st;
-    Staging &S = t_stage;
+    Staging &S = t_stage[current_device()];
     // the device staging buffer comes from s's pool: uploads wait for it
     MELA_CUDA_TRY(cudaEventRecord(S.fence, s));
     MELA_CUDA_TRY(cudaStreamWaitEvent(sin, S.fence, 0));

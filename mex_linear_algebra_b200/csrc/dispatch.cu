@@ -249,11 +249,40 @@ static int choose_unmeasured(int op, double m, double n, double p, double cells,
     return pick;
 }
 
+// The calling thread's recent pre-data decisions, by (op, shape) and model
+// generation: repeated shapes skip the model evaluation.
+namespace {
+struct PlanEntry {
+    unsigned gen;
+    int op, pick;
+    bool measure;
+    double m, n, p;
+};
+constexpr int kPlanCache = 256;
+thread_local PlanEntry t_plans[kPlanCache];
+}  // namespace
+
+static int choose_unmeasured_cached(int op, double m, double n, double p, double cells, bool *measure)
+{
+    const unsigned gen = costmodel_generation();
+    const unsigned long long h = ((unsigned long long)op * 0x9E3779B97F4A7C15ull) ^
+                                 ((unsigned long long)m * 0xBF58476D1CE4E5B9ull) ^
+                                 ((unsigned long long)n * 0x94D049BB133111EBull) ^ (unsigned long long)p;
+    PlanEntry &e = t_plans[(h ^ (h >> 29)) % kPlanCache];
+    if (e.gen == gen && e.op == op && e.m == m && e.n == n && e.p == p) {
+        *measure = e.measure;
+        return e.pick;
+    }
+    const int pick = choose_unmeasured(op, m, n, p, cells, measure);
+    if (pick >= 0) e = PlanEntry{gen, op, pick, *measure, m, n, p};
+    return pick;
+}
+
 static int choose_measuring(int op, double m, double n, double p, double cells,
                             const u64 *M, i64 ld, i64 rows, i64 cols, cudaStream_t s)
 {
     bool measure = false;
-    const int pick = choose_unmeasured(op, m, n, p, cells, &measure);
+    const int pick = choose_unmeasured_cached(op, m, n, p, cells, &measure);
     t_last_density = -1.0;
     if (pick < 0 || !measure) return pick;
     const double d = measure_density(M, ld, rows, cols, s);

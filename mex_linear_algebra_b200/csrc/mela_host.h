@@ -63,6 +63,8 @@ double measure_density(const u64 *M, i64 ld, i64 m, i64 n, cudaStream_t s);
 // Learned cost model (mlp.cu): configuration index for the request, or -1
 // without a model.
 bool costmodel_loaded();
+// Changes whenever a model is installed or removed (dispatch caches key on it).
+unsigned costmodel_generation();
 int costmodel_choose(int op, double m, double n, double p, double density, double batch_count,
                      double batch_log2_cells);
 // Predicted log2 microseconds of every configuration of the request

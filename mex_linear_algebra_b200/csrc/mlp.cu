@@ -13,6 +13,7 @@
 // Kernels: forward (one thread per sample), backward (one thread per sample,
 // per-block gradient sums in shared memory, then one global atomic per
 // parameter and block), Adam update (one thread per parameter).
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -170,6 +171,9 @@ struct CostModelWeights {
 };
 static std::mutex g_cm_mu;
 static std::shared_ptr<const CostModelWeights> g_cm;
+static std::atomic<unsigned> g_cm_generation{1};  // bumped on every install or removal
+
+unsigned costmodel_generation() { return g_cm_generation.load(std::memory_order_acquire); }
 
 static std::shared_ptr<const CostModelWeights> current_model()
 {
@@ -374,6 +378,7 @@ extern "C" mela_status mela_costmodel_load(const float *h_params)
     }
     std::lock_guard<std::mutex> g(g_cm_mu);
     g_cm = std::move(w);
+    g_cm_generation.fetch_add(1, std::memory_order_acq_rel);
     return MELA_OK;
 }
 
