@@ -196,3 +196,24 @@ def test_dispatch_plan_before_the_data():
         assert names[got] == want or abs(loss[names[got]] - loss[want]) < 1e-3 * max(1.0, loss[want]), (r, want)
         assert meas.value == int(loss[names[got]] > 15.0)
 
+
+
+def test_request_generators_and_stratified_sampling():
+    """The timing database's request sources: the size-stratified pick keeps
+    the largest requests, and the batch requests stay within their bounds."""
+    from mex_linear_algebra_b200 import autotune, gen
+    window = gen.mixed_stream(100000 + 5000, 4)[100000:]
+    pick = autotune.stratified(window, 240, bins=12)
+    size = lambda r: r["m"] * r["n"] + (r["n"] * r["p"] if r["op"] == "matmul" else 0)
+    assert 200 <= len(pick) <= 240
+    lw = np.log2([size(r) for r in window])
+    top_edge = lw.max() - (lw.max() - lw.min()) / 12
+    assert np.log2(max(size(r) for r in pick)) >= top_edge                # the largest bin is sampled
+    lg = np.log2([size(r) for r in pick])
+    assert np.mean(lg > np.median(np.log2([size(r) for r in window]))) > 0.5  # tilted toward large
+    for r in gen.batch_requests_sparse(200, 4, 7):
+        assert 48 <= r["m"] <= 600 and 1.5 * r["m"] - 1 <= r["n"] <= 2.5 * r["m"] + 1
+        assert 0.003 <= r["density"] <= 0.1 and r["batch_count"] in (1024, 4096, 16384)
+        assert r["batch_count"] == 1024 or r["batch_count"] * r["m"] * r["n"] <= (1 << 31)
+    for r in gen.batch_requests(200, 4, 7):
+        assert 32 <= r["m"] <= 1024 and r["batch_count"] in (64, 256, 1024, 4096)
