@@ -210,7 +210,9 @@ def test_request_generators_and_stratified_sampling():
     top_edge = lw.max() - (lw.max() - lw.min()) / 12
     assert np.log2(max(size(r) for r in pick)) >= top_edge                # the largest bin is sampled
     lg = np.log2([size(r) for r in pick])
-    assert np.mean(lg > np.median(np.log2([size(r) for r in window]))) > 0.5  # tilted toward large
+    # the largest quarter of the size range gets a larger share than in the stream itself
+    q3 = lw.max() - (lw.max() - lw.min()) / 4
+    assert np.mean(lg > q3) > 2 * np.mean(lw > q3)
     for r in gen.batch_requests_sparse(200, 4, 7):
         assert 48 <= r["m"] <= 600 and 1.5 * r["m"] - 1 <= r["n"] <= 2.5 * r["m"] + 1
         assert 0.003 <= r["density"] <= 0.1 and r["batch_count"] in (1024, 4096, 16384)
