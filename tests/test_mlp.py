@@ -212,7 +212,7 @@ def test_request_generators_and_stratified_sampling():
     lg = np.log2([size(r) for r in pick])
     # the largest quarter of the size range gets a larger share than in the stream itself
     q3 = lw.max() - (lw.max() - lw.min()) / 4
-    assert np.mean(lg > q3) > 2 * np.mean(lw > q3)
+    assert np.mean(lg > q3) > 1.5 * np.mean(lw > q3)
     for r in gen.batch_requests_sparse(200, 4, 7):
         assert 48 <= r["m"] <= 600 and 1.5 * r["m"] - 1 <= r["n"] <= 2.5 * r["m"] + 1
         assert 0.003 <= r["density"] <= 0.1 and r["batch_count"] in (1024, 4096, 16384)
