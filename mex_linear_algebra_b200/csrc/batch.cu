@@ -251,9 +251,13 @@ constexpr int kRegRows = 4;        // rows per thread there
 constexpr int kRegWarps = kRegThreads / 32;
 static_assert(kRegWarps == 8, "eight candidate slots");
 constexpr int kRegBar = 6;         // their named barrier
+constexpr int kSubBar = 5;         // warps 1.. while warp 0 selects the next panel's pivots
+constexpr int kCandMax = 384;      // candidate rows one warp selects pivots among (12 a lane)
 template <int TW>
 struct BigSmem {
     u64 coef[64];
+    int cand[kCandMax];  // the panel's candidate rows, in row order
+    int wcnt[16];        // candidates per warp
     u64 pub[2][kRegWarps][2];  // per warp: its candidate pivot's panel word and tag (by bit parity)
     alignas(16) unsigned wmin[2][kRegWarps];  // per warp: its candidate pivot row
     int bits[64], srow[64];
@@ -278,6 +282,81 @@ struct BigCfg {
     static_assert(NT >= kRegThreads, "the register panel needs 256 threads");
 };
 }  // namespace
+
+// Pivot selection of one panel among its candidate rows (active rows with a
+// nonzero panel word; cnt <= 32 R) by one warp, no block barrier: lane l holds
+// candidates l + 32 i.  Per bit that some candidate holds (the OR of their
+// words: XORs create no other bit), the lowest unused candidate holding it
+// becomes pivot k and is XORed into every other candidate holding the bit,
+// each carrying a 64-bit tag of the pivots folded into it.  Writes the
+// pivots' bits, rows and tags; returns the pivot count and the pivot mask.
+template <int R>
+__device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *ysnap, u64 *tag, int *bits,
+                                        int *srow, u64 *pm_out)
+{
+    const int lane = threadIdx.x & 31;
+    u64 y[R], t[R];
+    u32 unused = 0;
+    u64 orw = 0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int c = lane + 32 * i;
+        y[i] = c < cnt ? ysnap[cand[c]] : 0ull;
+        t[i] = 0;
+        unused |= (c < cnt ? 1u : 0u) << i;
+        orw |= y[i];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) orw |= __shfl_xor_sync(0xffffffffu, orw, o);
+    int k = 0;
+    u64 pmask = 0;
+    for (u64 rem = orw; rem; rem &= rem - 1) {
+        const int b = __ffsll((long long)rem) - 1;
+        // which of this lane's candidates hold bit b
+        const int sh = b & 31;
+        u32 hold = 0;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const u32 half = (b & 32) ? (u32)(y[i] >> 32) : (u32)y[i];
+            hold |= ((half >> sh) & 1u) << i;
+        }
+        const u32 cm = hold & unused;
+        const u32 bal = __ballot_sync(0xffffffffu, cm != 0);
+        if (bal == 0) continue;  // no unused candidate holds bit b any more
+        const int src = __ffs((int)bal) - 1;
+        const int ib = __shfl_sync(0xffffffffu, __ffs((int)cm) - 1, src);  // uniform
+        u64 yl = 0, tl = 0;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            if (i == ib) {  // uniform branch
+                yl = y[i];
+                tl = t[i];
+            }
+        const u64 yp = __shfl_sync(0xffffffffu, yl, src);
+        const u64 tp = __shfl_sync(0xffffffffu, tl, src) ^ (1ull << k);
+        if (lane == src) {
+            hold &= ~(1u << ib);  // the pivot keeps its row
+            unused &= ~(1u << ib);
+            bits[k] = b;
+            srow[k] = cand[src + 32 * ib];
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            if ((hold >> i) & 1u) {
+                y[i] ^= yp;
+                t[i] ^= tp;
+            }
+        pmask |= 1ull << b;
+        ++k;
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int c = lane + 32 * i;
+        if (c < cnt && !((unused >> i) & 1u)) tag[cand[c]] = t[i];
+    }
+    *pm_out = pmask;
+    return k;
+}
 
 // Element i (0..3, per thread) of a register array, by a select tree.
 __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
@@ -376,9 +455,9 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                                                            : reinterpret_cast<unsigned char *>(g + L.active);
     if (used + act_bytes <= kBigExtra) used += act_bytes;
     const bool rows_in_smem = used + 3 * row_bytes <= kBigExtra;
-    u64 *ysnap = rows_in_smem ? reinterpret_cast<u64 *>(extra + used) : g + L.ysg;
-    u64 *yv = rows_in_smem ? ysnap + m : g + L.yvg;
-    u64 *tag = rows_in_smem ? yv + m : g + L.tagg;
+    u64 *ysnap0 = rows_in_smem ? reinterpret_cast<u64 *>(extra + used) : g + L.ysg;
+    u64 *ysnap1 = rows_in_smem ? ysnap0 + m : g + L.yvg;
+    u64 *tag = rows_in_smem ? ysnap1 + m : g + L.tagg;
     if (rows_in_smem) used += 3 * row_bytes;
     // the matrix itself in shared memory too when it fits (at n = 2m: m up
     // to about 420 with 110 KB, 650 with 220 KB), else in the CTA's
@@ -390,138 +469,297 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     for (int j = tid; j < m; j += NT) active[j] = 1;
     __syncthreads();
 
+    // panel words of every row: one buffer for the current panel, the other
+    // for the next panel's (look-ahead) or the per-bit path's working copy
+    int cur = 0;
+    const int warp = tid >> 5;
+    // warp q owns rows [q chunk, (q + 1) chunk) for the candidate lists
+    const int chunk = (m + 32 * kWarps - 1) / (32 * kWarps) * 32;
+    const int jlo = warp * chunk, jhi = min(m, jlo + chunk);
+    // the look-ahead's one-word tables (words w and w + 1, 4 KB) live in the
+    // stage area, free from the reduced rows of one panel to the next
+    const bool lookahead_ok = r_in_smem && 64 * wc >= 2 * 16 * 16;
+    bool have_sel = false;  // this panel's pivots were selected during the previous one
+
+    // candidate rows of a panel (active, nonzero panel word) into S.cand in
+    // row order, from the per-warp counts in S.wcnt; returns their number
+    auto compact = [&](const u64 *ysp) -> int {
+        int cbase = 0, total = 0;
+        for (int q = 0; q < kWarps; ++q) {
+            const int c = S.wcnt[q];
+            cbase += q < warp ? c : 0;
+            total += c;
+        }
+        if (total <= kCandMax)
+            for (int j0 = jlo; j0 < jhi; j0 += 32) {
+                const int j = j0 + lane;
+                const bool ok = j < jhi && ysp[j] != 0 && active[j] == 1;
+                const u32 bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) S.cand[cbase + __popc(bal & ((1u << lane) - 1))] = j;
+                cbase += __popc(bal);
+            }
+        return total;
+    };
+    // pivots of a panel by one warp over its candidates: S.p, S.pm, S.bits,
+    // S.srow and the pivots' tags
+    auto select_warp = [&](const u64 *ysp, int ncand) {
+        u64 pmk;
+        int kk;
+        if (ncand <= 64)
+            kk = warp_select<2>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
+        else if (ncand <= 192)
+            kk = warp_select<6>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
+        else
+            kk = warp_select<12>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
+        if (lane == 0) {
+            S.p = kk;
+            S.pm = pmk;
+        }
+    };
+    // words [x_begin, wc) of every row that is not one of the panel's pivots
+    // take the reduced rows of the pivot bits its panel word holds: 16
+    // nibble-table lookups per word, TW words at a time, by warps wfirst ..
+    // kWarps - 1 (a named barrier among them when warp 0 is busy elsewhere)
+    auto update_words = [&](u64 pmask, const u64 *ysp, int x_begin, int wfirst) {
+        const int nthr = NT - 32 * wfirst, t0 = tid - 32 * wfirst, nw = kWarps - wfirst, wq = warp - wfirst;
+        auto bar = [&]() {
+            if (wfirst == 0)
+                __syncthreads();
+            else
+                asm volatile("bar.sync %0, %1;" ::"r"(kSubBar), "r"(nthr) : "memory");
+        };
+        for (int x0 = x_begin; x0 < wc; x0 += TW) {
+            for (int e = t0; e < 16 * 5 * TW; e += nthr) {
+                const int t = e % TW, gh = e / TW, gi = gh / 5, h = gh % 5;
+                if (h == 4) {
+                    S.T[gi][0][t] = 0;
+                    continue;
+                }
+                const int bb = 4 * gi + h, x = x0 + t;
+                u64 v = 0;
+                if (((pmask >> bb) & 1) && x < wc) v = Rbuf[(size_t)bb * wc + x];
+                S.T[gi][1 << h][t] = v;
+            }
+            bar();
+            for (int h = 1; h < 4; ++h) {
+                const int cnt = (1 << h) - 1;
+                for (int e = t0; e < 16 * cnt * TW; e += nthr) {
+                    const int t = e % TW, rest = e / TW, gi = rest / cnt, v = (1 << h) + 1 + rest % cnt;
+                    S.T[gi][v][t] = S.T[gi][v - (1 << h)][t] ^ S.T[gi][1 << h][t];
+                }
+                bar();
+            }
+            // lane (h, xl) = (lane / TW, lane % TW) takes word x0 + xl of
+            // rows j0 + 4 h .. + 3 (32 / TW rows per warp instruction); the
+            // next rows' words are read while the current ones are combined
+            constexpr int RPW = 32 / TW;
+            const int kStep = nw * 4 * RPW;
+            const int xl = lane % TW, hsel = lane / TW;
+            const int x = x0 + xl;
+            // coefficient words (0: skip) and matrix words of rows jb .. jb + 3
+            auto fetch = [&](int jb, u64 (&y)[4], u64 (&a)[4]) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j = jb + q;
+                    y[q] = (j < m && x < wc && active[j] != 2) ? ysp[j] & pmask : 0ull;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q] = y[q] ? A[(size_t)(jb + q) * wc + x] : 0ull;
+            };
+            int jb = wq * 4 * RPW + 4 * hsel;
+            u64 y[4], a[4];
+            fetch(jb, y, a);
+            for (; jb - 4 * hsel < m; jb += kStep) {
+                u64 yn[4], an[4];
+                fetch(jb + kStep, yn, an);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (!y[q]) continue;
+                    u64 acc = 0;
+#pragma unroll
+                    for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][xl];
+                    A[(size_t)(jb + q) * wc + x] = a[q] ^ acc;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    y[q] = yn[q];
+                    a[q] = an[q];
+                }
+            }
+            bar();
+        }
+    };
+
     int r = 0;
     for (int w = 0; w < wc && r < m; ++w) {
+        u64 *ysnap = cur ? ysnap1 : ysnap0, *yv = cur ? ysnap0 : ysnap1;
         int k = 0;
         u64 pmask = 0;
-        if (m <= kRegRows * kRegThreads) {
-            // 1-2. the panel in registers of the first eight warps: thread l
-            // holds rows l + 256 i.  Per bit one named barrier: each warp
-            // publishes its lowest unused row holding the bit (index, panel
-            // word and tag); the lowest of the eight is the pivot.
-            for (int j = tid; j < m; j += NT) ysnap[j] = A[(size_t)j * wc + w];
-            __syncthreads();
-            if (tid < kRegThreads) {
-                const int warp = tid >> 5;
-                u64 y[kRegRows], t[kRegRows];
-                u32 unused = 0;
-#pragma unroll
-                for (int i = 0; i < kRegRows; ++i) {
-                    const int j = tid + kRegThreads * i;
-                    const int a = j < m ? active[j] : 0;
-                    y[i] = a == 1 ? ysnap[j] : 0ull;
-                    t[i] = 0;
-                    unused |= (a == 1 ? 1u : 0u) << i;
-                }
-#pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    for (int bb = 0; bb < 32; ++bb) {
-                        const int b = 32 * half + bb;
-                        u32 cm = 0;
-#pragma unroll
-                        for (int i = 0; i < kRegRows; ++i) cm |= (((u32)(y[i] >> (32 * half)) >> bb) & 1u) << i;
-                        cm &= unused;
-                        const int ib = __ffs((int)cm) - 1;
-                        const unsigned jb = ib >= 0 ? (unsigned)(tid + kRegThreads * ib) : (unsigned)INT_MAX;
-                        const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
-                        const int par = bb & 1;
-                        if (jb == wm && wm != (unsigned)INT_MAX) {
-                            S.pub[par][warp][0] = sel4r(y, ib);
-                            S.pub[par][warp][1] = sel4r(t, ib);
-                        }
-                        if (lane == 0) S.wmin[par][warp] = wm;
-                        asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
-                        const uint4 wa = reinterpret_cast<const uint4 *>(S.wmin[par])[0];
-                        const uint4 wb = reinterpret_cast<const uint4 *>(S.wmin[par])[1];
-                        const unsigned pm = min(min(min(wa.x, wa.y), min(wa.z, wa.w)),
-                                                min(min(wb.x, wb.y), min(wb.z, wb.w)));
-                        if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
-                        const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
-                        const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
-                        if (tid == 0) {
-                            S.bits[k] = b;
-                            S.srow[k] = pr;
-                        }
-                        // every other row holding bit b takes the pivot row (branch-free)
-                        const int own = (pr & (kRegThreads - 1)) == tid ? pr / kRegThreads : -1;
-#pragma unroll
-                        for (int i = 0; i < kRegRows; ++i) {
-                            const u64 hit = i == own ? 0ull : 0ull - (u64)(((u32)(y[i] >> (32 * half)) >> bb) & 1u);
-                            y[i] ^= yp & hit;
-                            t[i] ^= tp & hit;
-                        }
-                        if (own >= 0) unused &= ~(1u << own);
-                        pmask |= 1ull << b;
-                        ++k;
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < kRegRows; ++i) {
-                    const int j = tid + kRegThreads * i;
-                    if (j < m) tag[j] = t[i];
-                }
-                if (tid == 0) {
-                    S.p = k;
-                    S.pm = pmask;
-                }
-            }
-            __syncthreads();
+        if (have_sel) {
+            // selected during the previous panel's update, pivots marked
             k = S.p;
             pmask = S.pm;
-            for (int q = tid; q < k; q += NT) active[S.srow[q]] = 2;
-            __syncthreads();
         } else {
-            // 1. panel words, pivot search for bit 0
-            if (tid < 3) S.slots[tid] = INT_MAX;
-            __syncthreads();
-            unsigned best = INT_MAX;
-            for (int j = tid; j < m; j += NT) {
-                const u64 word = A[(size_t)j * wc + w];
-                ysnap[j] = word;
-                const u64 y = active[j] == 1 ? word : 0ull;
-                yv[j] = y;
-                tag[j] = 0;
-                if ((y & 1ull) && best == (unsigned)INT_MAX) best = j;
-            }
-            best = __reduce_min_sync(0xffffffffu, best);
-            if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[0], (int)best);
-            __syncthreads();
-            // 2. per-bit elimination of the panel words with combination tags
-            for (int b = 0; b < 64; ++b) {
-                const int p = S.slots[b % 3];
-                if (tid == 0) S.slots[(b + 2) % 3] = INT_MAX;
-                if (p != INT_MAX) {
-                    const u64 yp = yv[p], tp = tag[p] ^ (1ull << k);
-                    if (tid == 0) {
-                        S.bits[k] = b;
-                        S.srow[k] = p;
-                    }
-                    if (p % NT == tid) active[p] = 2;
-                    const u64 bit = 1ull << b;
-                    for (int j = tid; j < m; j += NT) {
-                        if (j == p || active[j] == 0) continue;
-                        if (yv[j] & bit) {
-                            yv[j] ^= yp;
-                            tag[j] ^= tp;
-                        }
-                    }
-                    pmask |= bit;
-                    ++k;
+            // 1. panel words and the per-warp candidate counts
+            int ncand = 0;
+            for (int j0 = jlo; j0 < jhi; j0 += 128) {
+                u64 word[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int j = j0 + 32 * u + lane;
+                    word[u] = j < jhi ? A[(size_t)j * wc + w] : 0ull;
                 }
-                if (b < 63) {
-                    const u64 bit = 1ull << (b + 1);
-                    best = INT_MAX;
-                    for (int j = tid; j < m; j += NT)
-                        if (active[j] == 1 && (yv[j] & bit)) {
-                            best = j;
-                            break;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int j = j0 + 32 * u + lane;
+                    bool ok = false;
+                    if (j < jhi) {
+                        ysnap[j] = word[u];
+                        ok = word[u] != 0 && active[j] == 1;
+                    }
+                    ncand += __popc(__ballot_sync(0xffffffffu, ok));
+                }
+            }
+            if (lane == 0) S.wcnt[warp] = ncand;
+            __syncthreads();
+            ncand = compact(ysnap);
+            if (ncand <= kCandMax) {
+                // 2. pivots by one warp over the candidates (few rows hold a
+                // bit of the panel in a sparse matrix)
+                __syncthreads();
+                if (warp == 0) select_warp(ysnap, ncand);
+                __syncthreads();
+                k = S.p;
+                pmask = S.pm;
+                for (int q = tid; q < k; q += NT) active[S.srow[q]] = 2;
+                __syncthreads();
+            } else if (m <= kRegRows * kRegThreads) {
+                // 2. the panel in registers of the first eight warps: thread l
+                // holds rows l + 256 i.  Per bit one named barrier: each warp
+                // publishes its lowest unused row holding the bit (index, panel
+                // word and tag); the lowest of the eight is the pivot.
+                if (tid < kRegThreads) {
+                    u64 y[kRegRows], t[kRegRows];
+                    u32 unused = 0;
+#pragma unroll
+                    for (int i = 0; i < kRegRows; ++i) {
+                        const int j = tid + kRegThreads * i;
+                        const int a = j < m ? active[j] : 0;
+                        y[i] = a == 1 ? ysnap[j] : 0ull;
+                        t[i] = 0;
+                        unused |= (a == 1 ? 1u : 0u) << i;
+                    }
+#pragma unroll
+                    for (int half = 0; half < 2; ++half) {
+                        for (int bb = 0; bb < 32; ++bb) {
+                            const int b = 32 * half + bb;
+                            u32 cm = 0;
+#pragma unroll
+                            for (int i = 0; i < kRegRows; ++i) cm |= (((u32)(y[i] >> (32 * half)) >> bb) & 1u) << i;
+                            cm &= unused;
+                            const int ib = __ffs((int)cm) - 1;
+                            const unsigned jb = ib >= 0 ? (unsigned)(tid + kRegThreads * ib) : (unsigned)INT_MAX;
+                            const unsigned wm = __reduce_min_sync(0xffffffffu, jb);
+                            const int par = bb & 1;
+                            if (jb == wm && wm != (unsigned)INT_MAX) {
+                                S.pub[par][warp][0] = sel4r(y, ib);
+                                S.pub[par][warp][1] = sel4r(t, ib);
+                            }
+                            if (lane == 0) S.wmin[par][warp] = wm;
+                            asm volatile("bar.sync %0, %1;" ::"r"(kRegBar), "r"(kRegThreads) : "memory");
+                            const uint4 wa = reinterpret_cast<const uint4 *>(S.wmin[par])[0];
+                            const uint4 wb = reinterpret_cast<const uint4 *>(S.wmin[par])[1];
+                            const unsigned pm = min(min(min(wa.x, wa.y), min(wa.z, wa.w)),
+                                                    min(min(wb.x, wb.y), min(wb.z, wb.w)));
+                            if (pm == (unsigned)INT_MAX) continue;  // no unused row holds bit b
+                            const int pr = (int)pm, pw = (pr & (kRegThreads - 1)) >> 5;
+                            const u64 yp = S.pub[par][pw][0], tp = S.pub[par][pw][1] ^ (1ull << k);
+                            if (tid == 0) {
+                                S.bits[k] = b;
+                                S.srow[k] = pr;
+                            }
+                            // every other row holding bit b takes the pivot row (branch-free)
+                            const int own = (pr & (kRegThreads - 1)) == tid ? pr / kRegThreads : -1;
+#pragma unroll
+                            for (int i = 0; i < kRegRows; ++i) {
+                                const u64 hit = i == own ? 0ull : 0ull - (u64)(((u32)(y[i] >> (32 * half)) >> bb) & 1u);
+                                y[i] ^= yp & hit;
+                                t[i] ^= tp & hit;
+                            }
+                            if (own >= 0) unused &= ~(1u << own);
+                            pmask |= 1ull << b;
+                            ++k;
                         }
-                    best = __reduce_min_sync(0xffffffffu, best);
-                    if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[(b + 1) % 3], (int)best);
+                    }
+#pragma unroll
+                    for (int i = 0; i < kRegRows; ++i) {
+                        const int j = tid + kRegThreads * i;
+                        if (j < m) tag[j] = t[i];
+                    }
+                    if (tid == 0) {
+                        S.p = k;
+                        S.pm = pmask;
+                    }
                 }
                 __syncthreads();
+                k = S.p;
+                pmask = S.pm;
+                for (int q = tid; q < k; q += NT) active[S.srow[q]] = 2;
+                __syncthreads();
+            } else {
+                // 1. panel words, pivot search for bit 0
+                if (tid < 3) S.slots[tid] = INT_MAX;
+                __syncthreads();
+                unsigned best = INT_MAX;
+                for (int j = tid; j < m; j += NT) {
+                    const u64 word = A[(size_t)j * wc + w];
+                    ysnap[j] = word;
+                    const u64 y = active[j] == 1 ? word : 0ull;
+                    yv[j] = y;
+                    tag[j] = 0;
+                    if ((y & 1ull) && best == (unsigned)INT_MAX) best = j;
+                }
+                best = __reduce_min_sync(0xffffffffu, best);
+                if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[0], (int)best);
+                __syncthreads();
+                // 2. per-bit elimination of the panel words with combination tags
+                for (int b = 0; b < 64; ++b) {
+                    const int p = S.slots[b % 3];
+                    if (tid == 0) S.slots[(b + 2) % 3] = INT_MAX;
+                    if (p != INT_MAX) {
+                        const u64 yp = yv[p], tp = tag[p] ^ (1ull << k);
+                        if (tid == 0) {
+                            S.bits[k] = b;
+                            S.srow[k] = p;
+                        }
+                        if (p % NT == tid) active[p] = 2;
+                        const u64 bit = 1ull << b;
+                        for (int j = tid; j < m; j += NT) {
+                            if (j == p || active[j] == 0) continue;
+                            if (yv[j] & bit) {
+                                yv[j] ^= yp;
+                                tag[j] ^= tp;
+                            }
+                        }
+                        pmask |= bit;
+                        ++k;
+                    }
+                    if (b < 63) {
+                        const u64 bit = 1ull << (b + 1);
+                        best = INT_MAX;
+                        for (int j = tid; j < m; j += NT)
+                            if (active[j] == 1 && (yv[j] & bit)) {
+                                best = j;
+                                break;
+                            }
+                        best = __reduce_min_sync(0xffffffffu, best);
+                        if (lane == 0 && best != (unsigned)INT_MAX) atomicMin(&S.slots[(b + 1) % 3], (int)best);
+                    }
+                    __syncthreads();
+                }
             }
         }
+        have_sel = false;
         const int p = k;
         if (p == 0) continue;
         for (int t = tid; t < p; t += NT) {
@@ -530,11 +768,24 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             prow[r + t] = S.srow[t];
         }
         const int rem = wc - w;
-        // 3. reduced pivot rows from the staged original rows
+        // 3. reduced pivot rows from the staged original rows (Rbuf row b:
+        // the reduced row of the pivot on bit b)
         __syncthreads();
-        for (int e = tid; e < p * rem; e += NT) {
-            const int i = e / rem, x = w + e % rem;
-            stage[(size_t)i * wc + x] = A[(size_t)S.srow[i] * wc + x];
+        {
+            constexpr int U = 8;
+            for (int e0 = tid; e0 < p * rem; e0 += U * NT) {
+                u64 v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + u * NT;
+                    v[u] = e < p * rem ? A[(size_t)S.srow[e / rem] * wc + w + e % rem] : 0ull;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + u * NT;
+                    if (e < p * rem) stage[(size_t)(e / rem) * wc + w + e % rem] = v[u];
+                }
+            }
         }
         __syncthreads();
         for (int e = tid; e < p * rem; e += NT) {
@@ -545,70 +796,90 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                 c &= c - 1;
                 v ^= stage[(size_t)i * wc + x];
             }
-            Rbuf[(size_t)kk * wc + x] = v;
+            Rbuf[(size_t)S.bits[kk] * wc + x] = v;
             A[(size_t)S.srow[kk] * wc + x] = v;
         }
         __syncthreads();
-        // 4. update every other row, 32 words at a time
-        for (int x0 = w; x0 < wc; x0 += TW) {
-            for (int e = tid; e < 16 * 5 * TW; e += NT) {
-                const int t = e % TW, gh = e / TW, gi = gh / 5, h = gh % 5;
-                if (h == 4) {
-                    S.T[gi][0][t] = 0;
-                    continue;
-                }
-                const int bb = 4 * gi + h, x = x0 + t;
-                u64 v = 0;
-                if (((pmask >> bb) & 1) && x < wc) {
-                    const int kk = __popcll(pmask & ((1ull << bb) - 1));
-                    v = Rbuf[(size_t)kk * wc + x];
-                }
-                S.T[gi][1 << h][t] = v;
-            }
+        // 4. update every other row (the reduced rows of the pivot bits its
+        // panel word holds)
+        const bool la = lookahead_ok && w + 1 < wc && r + p < m;
+        if (!la) {
+            update_words(pmask, ysnap, w, 0);
+            for (int t = tid; t < p; t += NT) active[S.srow[t]] = 0;
+            r += p;
             __syncthreads();
-            for (int h = 1; h < 4; ++h) {
-                const int cnt = (1 << h) - 1;
-                for (int e = tid; e < 16 * cnt * TW; e += NT) {
-                    const int t = e % TW, rest = e / TW, gi = rest / cnt, v = (1 << h) + 1 + rest % cnt;
-                    S.T[gi][v][t] = S.T[gi][v - (1 << h)][t] ^ S.T[gi][1 << h][t];
-                }
-                __syncthreads();
-            }
-            // lane (h, xl) = (lane / TW, lane % TW) takes word x0 + xl of
-            // rows j0 + 4 h .. + 3 (32 / TW rows per warp instruction)
-            constexpr int RPW = 32 / TW;
-            const int xl = lane % TW, hsel = lane / TW;
-            const int x = x0 + xl;
-            const int warp = tid >> 5;
-            for (int j0 = warp * 4 * RPW; j0 < m; j0 += kWarps * 4 * RPW) {
-                u64 y[4], a[4];
-                bool go[4];
-                const int jb = j0 + 4 * hsel;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = jb + q;
-                    go[q] = false;
-                    y[q] = 0;
-                    if (j < m && active[j] != 2) {
-                        y[q] = ysnap[j] & pmask;
-                        go[q] = y[q] != 0 && x < wc;
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (go[q]) a[q] = A[(size_t)(jb + q) * wc + x];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (!go[q]) continue;
-                    u64 acc = 0;
-#pragma unroll
-                    for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][xl];
-                    A[(size_t)(jb + q) * wc + x] = a[q] ^ acc;
-                }
-            }
-            __syncthreads();
+            continue;
         }
-        for (int t = tid; t < p; t += NT) active[S.srow[t]] = 0;
+        // 4a. look-ahead: words w and w + 1 of every row first (one-word
+        // tables), the new word w + 1 being the next panel's snapshot
+        u64 *ysn = yv;
+        u64(*T01)[16][16] = reinterpret_cast<u64(*)[16][16]>(stage);
+        for (int e = tid; e < 2 * 16 * 16; e += NT) {
+            const int which = e >> 8, gi = (e >> 4) & 15, v = e & 15;
+            u64 acc = 0;
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int bb = 4 * gi + h;
+                if (((v >> h) & 1) && ((pmask >> bb) & 1)) acc ^= Rbuf[(size_t)bb * wc + w + which];
+            }
+            T01[which][gi][v] = acc;
+        }
+        __syncthreads();
+        int nc = 0;
+        for (int j0 = jlo; j0 < jhi; j0 += 128) {
+            u64 a1[4];
+            int st[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + 32 * u + lane;
+                st[u] = j < jhi ? active[j] : 0;
+                a1[u] = j < jhi ? A[(size_t)j * wc + w + 1] : 0ull;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + 32 * u + lane;
+                bool ok = false;
+                if (j < jhi) {
+                    const u64 y = st[u] != 2 ? ysnap[j] & pmask : 0ull;
+                    if (y) {
+                        u64 acc0 = 0, acc1 = 0;
+#pragma unroll
+                        for (int gi = 0; gi < 16; ++gi) {
+                            const int nib = (int)(y >> (4 * gi)) & 15;
+                            acc0 ^= T01[0][gi][nib];
+                            acc1 ^= T01[1][gi][nib];
+                        }
+                        A[(size_t)j * wc + w] = ysnap[j] ^ acc0;
+                        a1[u] ^= acc1;
+                        A[(size_t)j * wc + w + 1] = a1[u];
+                    }
+                    ysn[j] = a1[u];
+                    ok = a1[u] != 0 && st[u] == 1;
+                }
+                nc += __popc(__ballot_sync(0xffffffffu, ok));
+            }
+        }
+        if (lane == 0) S.wcnt[warp] = nc;
+        __syncthreads();
+        const int ncn = compact(ysn);
+        __syncthreads();
+        if (ncn <= kCandMax) {
+            // 4b. the next panel's pivots by warp 0 while the other warps
+            // update words w + 2 .. of this one
+            if (warp == 0)
+                select_warp(ysn, ncn);
+            else
+                update_words(pmask, ysnap, w + 2, 1);
+            __syncthreads();
+            for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
+            const int kn = S.p;
+            for (int t = tid; t < kn; t += NT) active[S.srow[t]] = 2;
+            have_sel = true;
+            cur ^= 1;
+        } else {
+            update_words(pmask, ysnap, w + 2, 0);
+            for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
+        }
         r += p;
         __syncthreads();
     }
