@@ -258,6 +258,7 @@ struct BigSmem {
     u64 coef[64];
     int cand[kCandMax];  // the panel's candidate rows, in row order
     int wcnt[16];        // candidates per warp
+    int ucnt[16];        // rows to update per warp
     u64 pub[2][kRegWarps][2];  // per warp: its candidate pivot's panel word and tag (by bit parity)
     alignas(16) unsigned wmin[2][kRegWarps];  // per warp: its candidate pivot row
     int bits[64], srow[64];
@@ -459,6 +460,10 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u64 *ysnap1 = rows_in_smem ? ysnap0 + m : g + L.yvg;
     u64 *tag = rows_in_smem ? ysnap1 + m : g + L.tagg;
     if (rows_in_smem) used += 3 * row_bytes;
+    // the look-ahead's list of rows to update (row order), when it fits
+    const size_t ul_bytes = ((size_t)m * 4 + 15) & ~(size_t)15;
+    int *ulist = rows_in_smem && used + ul_bytes <= kBigExtra ? reinterpret_cast<int *>(extra + used) : nullptr;
+    if (ulist) used += ul_bytes;
     // the matrix itself in shared memory too when it fits (at n = 2m: m up
     // to about 420 with 110 KB, 650 with 220 KB), else in the CTA's
     // L2-resident scratch
@@ -520,7 +525,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     // take the reduced rows of the pivot bits its panel word holds: 16
     // nibble-table lookups per word, TW words at a time, by warps wfirst ..
     // kWarps - 1 (a named barrier among them when warp 0 is busy elsewhere)
-    auto update_words = [&](u64 pmask, const u64 *ysp, int x_begin, int wfirst) {
+    auto update_words = [&](u64 pmask, const u64 *ysp, int x_begin, int wfirst, const int *ul, int nul) {
         const int nthr = NT - 32 * wfirst, t0 = tid - 32 * wfirst, nw = kWarps - wfirst, wq = warp - wfirst;
         auto bar = [&]() {
             if (wfirst == 0)
@@ -556,32 +561,40 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             const int kStep = nw * 4 * RPW;
             const int xl = lane % TW, hsel = lane / TW;
             const int x = x0 + xl;
-            // coefficient words (0: skip) and matrix words of rows jb .. jb + 3
-            auto fetch = [&](int jb, u64 (&y)[4], u64 (&a)[4]) {
+            // rows jb .. jb + 3 (or list entries jb .. jb + 3): their indices,
+            // coefficient words (0: skip) and matrix words
+            const int nrows = ul ? nul : m;
+            auto fetch = [&](int jb, int (&jr)[4], u64 (&y)[4], u64 (&a)[4]) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int j = jb + q;
-                    y[q] = (j < m && x < wc && active[j] != 2) ? ysp[j] & pmask : 0ull;
+                    const int i = jb + q;
+                    jr[q] = i < nrows ? (ul ? ul[i] : i) : -1;
                 }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = y[q] ? A[(size_t)(jb + q) * wc + x] : 0ull;
+                for (int q = 0; q < 4; ++q)
+                    y[q] = (jr[q] >= 0 && x < wc && (ul || active[jr[q]] != 2)) ? ysp[jr[q]] & pmask : 0ull;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q] = y[q] ? A[(size_t)jr[q] * wc + x] : 0ull;
             };
             int jb = wq * 4 * RPW + 4 * hsel;
+            int jr[4];
             u64 y[4], a[4];
-            fetch(jb, y, a);
-            for (; jb - 4 * hsel < m; jb += kStep) {
+            fetch(jb, jr, y, a);
+            for (; jb - 4 * hsel < nrows; jb += kStep) {
+                int jn[4];
                 u64 yn[4], an[4];
-                fetch(jb + kStep, yn, an);
+                fetch(jb + kStep, jn, yn, an);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (!y[q]) continue;
                     u64 acc = 0;
 #pragma unroll
                     for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(y[q] >> (4 * gi)) & 15][xl];
-                    A[(size_t)(jb + q) * wc + x] = a[q] ^ acc;
+                    A[(size_t)jr[q] * wc + x] = a[q] ^ acc;
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
+                    jr[q] = jn[q];
                     y[q] = yn[q];
                     a[q] = an[q];
                 }
@@ -804,7 +817,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         // panel word holds)
         const bool la = lookahead_ok && w + 1 < wc && r + p < m;
         if (!la) {
-            update_words(pmask, ysnap, w, 0);
+            update_words(pmask, ysnap, w, 0, nullptr, 0);
             for (int t = tid; t < p; t += NT) active[S.srow[t]] = 0;
             r += p;
             __syncthreads();
@@ -825,7 +838,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             T01[which][gi][v] = acc;
         }
         __syncthreads();
-        int nc = 0;
+        int nc = 0, nu = 0;
         for (int j0 = jlo; j0 < jhi; j0 += 128) {
             u64 a1[4];
             int st[4];
@@ -838,7 +851,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int j = j0 + 32 * u + lane;
-                bool ok = false;
+                bool ok = false, upd = false;
                 if (j < jhi) {
                     const u64 y = st[u] != 2 ? ysnap[j] & pmask : 0ull;
                     if (y) {
@@ -855,13 +868,35 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                     }
                     ysn[j] = a1[u];
                     ok = a1[u] != 0 && st[u] == 1;
+                    upd = y != 0;
                 }
                 nc += __popc(__ballot_sync(0xffffffffu, ok));
+                nu += __popc(__ballot_sync(0xffffffffu, upd));
             }
         }
-        if (lane == 0) S.wcnt[warp] = nc;
+        if (lane == 0) {
+            S.wcnt[warp] = nc;
+            S.ucnt[warp] = nu;
+        }
         __syncthreads();
         const int ncn = compact(ysn);
+        // the rows to update, in row order
+        int nul = 0;
+        if (ulist) {
+            int ubase = 0;
+            for (int q = 0; q < kWarps; ++q) {
+                const int c = S.ucnt[q];
+                ubase += q < warp ? c : 0;
+                nul += c;
+            }
+            for (int j0 = jlo; j0 < jhi; j0 += 32) {
+                const int j = j0 + lane;
+                const bool upd = j < jhi && active[j] != 2 && (ysnap[j] & pmask) != 0;
+                const u32 bal = __ballot_sync(0xffffffffu, upd);
+                if (upd) ulist[ubase + __popc(bal & ((1u << lane) - 1))] = j;
+                ubase += __popc(bal);
+            }
+        }
         __syncthreads();
         if (ncn <= kCandMax) {
             // 4b. the next panel's pivots by warp 0 while the other warps
@@ -869,7 +904,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             if (warp == 0)
                 select_warp(ysn, ncn);
             else
-                update_words(pmask, ysnap, w + 2, 1);
+                update_words(pmask, ysnap, w + 2, 1, ulist, nul);
             __syncthreads();
             for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
             const int kn = S.p;
@@ -877,7 +912,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             have_sel = true;
             cur ^= 1;
         } else {
-            update_words(pmask, ysnap, w + 2, 0);
+            update_words(pmask, ysnap, w + 2, 0, ulist, nul);
             for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
         }
         r += p;
