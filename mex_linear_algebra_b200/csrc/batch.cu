@@ -257,6 +257,7 @@ template <int TW>
 struct BigSmem {
     u64 coef[64];
     int cand[kCandMax];  // the panel's candidate rows, in row order
+    int prev_srow[64];   // the pivot rows of the panel being updated (look-ahead)
     int wcnt[16];        // candidates per warp
     int ucnt[16];        // rows to update per warp
     u64 pub[2][kRegWarps][2];  // per warp: its candidate pivot's panel word and tag (by bit parity)
@@ -284,19 +285,57 @@ struct BigCfg {
 };
 }  // namespace
 
+// v[i] for a lane-local index i < R (R <= 16) by a select tree: no local
+// memory and a dependence depth of four selects.
+template <int R>
+__device__ __forceinline__ u64 pick_reg(const u64 (&v)[R], int i)
+{
+    u64 a[8], b[4], c[2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const u64 lo = 2 * j < R ? v[2 * j] : 0ull, hi = 2 * j + 1 < R ? v[2 * j + 1] : 0ull;
+        a[j] = (i & 1) ? hi : lo;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = (i & 2) ? a[2 * j + 1] : a[2 * j];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) c[j] = (i & 4) ? b[2 * j + 1] : b[2 * j];
+    return (i & 8) ? c[1] : c[0];
+}
+
+// Bit b of each of a lane's R words, as an R-bit mask (four independent
+// partial masks, so that the dependence chain stays short).
+template <int R>
+__device__ __forceinline__ u32 bit_mask(const u64 (&y)[R], int b)
+{
+    const int sh = b & 31;
+    u32 h[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const u32 half = (b & 32) ? (u32)(y[i] >> 32) : (u32)y[i];
+        h[i & 3] |= ((half >> sh) & 1u) << i;
+    }
+    return (h[0] | h[1]) | (h[2] | h[3]);
+}
+
 // Pivot selection of one panel among its candidate rows (active rows with a
 // nonzero panel word; cnt <= 32 R) by one warp, no block barrier: lane l holds
 // candidates l + 32 i.  Per bit that some candidate holds (the OR of their
 // words: XORs create no other bit), the lowest unused candidate holding it
 // becomes pivot k and is XORed into every other candidate holding the bit,
-// each carrying a 64-bit tag of the pivots folded into it.  Writes the
-// pivots' bits, rows and tags; returns the pivot count and the pivot mask.
+// each carrying a 64-bit tag of the pivots folded into it.  A step's critical
+// path is a ballot and a shuffle: which rows hold the next bit is computed
+// from the words before the XOR (the bit flips in the rows that take the
+// pivot where the pivot word has it), and the pivots' bits are recorded in
+// registers and written out at the end.  Writes the pivots' bits, rows and
+// tags; returns the pivot count and the pivot mask.
 template <int R>
 __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *ysnap, u64 *tag, int *bits,
-                                        int *srow, u64 *pm_out)
+                                           int *srow, u64 *pm_out)
 {
     const int lane = threadIdx.x & 31;
     u64 y[R], t[R];
+    int pb[R];  // the bit a candidate became the pivot of, or -1
     u32 unused = 0;
     u64 orw = 0;
 #pragma unroll
@@ -304,6 +343,7 @@ __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *
         const int c = lane + 32 * i;
         y[i] = c < cnt ? ysnap[cand[c]] : 0ull;
         t[i] = 0;
+        pb[i] = -1;
         unused |= (c < cnt ? 1u : 0u) << i;
         orw |= y[i];
     }
@@ -311,50 +351,51 @@ __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *
     for (int o = 16; o; o >>= 1) orw |= __shfl_xor_sync(0xffffffffu, orw, o);
     int k = 0;
     u64 pmask = 0;
-    for (u64 rem = orw; rem; rem &= rem - 1) {
-        const int b = __ffsll((long long)rem) - 1;
-        // which of this lane's candidates hold bit b
-        const int sh = b & 31;
-        u32 hold = 0;
+    u64 rem = orw;
+    if (rem) {
+        int b = __ffsll((long long)rem) - 1;
+        u32 hold = bit_mask<R>(y, b);
+        while (true) {
+            const u64 rem_n = rem & (rem - 1);
+            const int bn = rem_n ? __ffsll((long long)rem_n) - 1 : 0;
+            u32 hold_n = bit_mask<R>(y, bn);
+            const u32 cm = hold & unused;
+            const u32 bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (bal) {
+                const int src = __ffs((int)bal) - 1;
+                const int ib = __ffs((int)cm) - 1;  // meaningful in lane src
+                const u64 yp = __shfl_sync(0xffffffffu, pick_reg<R>(y, ib), src);
+                const u64 tp = __shfl_sync(0xffffffffu, pick_reg<R>(t, ib), src) ^ (1ull << k);
+                const u32 me = lane == src ? (1u << ib) : 0u;
+                const u32 hit = hold & ~me;  // every other candidate holding bit b
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
-            const u32 half = (b & 32) ? (u32)(y[i] >> 32) : (u32)y[i];
-            hold |= ((half >> sh) & 1u) << i;
-        }
-        const u32 cm = hold & unused;
-        const u32 bal = __ballot_sync(0xffffffffu, cm != 0);
-        if (bal == 0) continue;  // no unused candidate holds bit b any more
-        const int src = __ffs((int)bal) - 1;
-        const int ib = __shfl_sync(0xffffffffu, __ffs((int)cm) - 1, src);  // uniform
-        u64 yl = 0, tl = 0;
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-            if (i == ib) {  // uniform branch
-                yl = y[i];
-                tl = t[i];
+                for (int i = 0; i < R; ++i) {
+                    if ((hit >> i) & 1u) {
+                        y[i] ^= yp;
+                        t[i] ^= tp;
+                    }
+                    if ((me >> i) & 1u) pb[i] = b;
+                }
+                unused &= ~me;
+                hold_n ^= ((yp >> bn) & 1ull) ? hit : 0u;
+                pmask |= 1ull << b;
+                ++k;
             }
-        const u64 yp = __shfl_sync(0xffffffffu, yl, src);
-        const u64 tp = __shfl_sync(0xffffffffu, tl, src) ^ (1ull << k);
-        if (lane == src) {
-            hold &= ~(1u << ib);  // the pivot keeps its row
-            unused &= ~(1u << ib);
-            bits[k] = b;
-            srow[k] = cand[src + 32 * ib];
+            if (!rem_n) break;
+            rem = rem_n;
+            b = bn;
+            hold = hold_n;
         }
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-            if ((hold >> i) & 1u) {
-                y[i] ^= yp;
-                t[i] ^= tp;
-            }
-        pmask |= 1ull << b;
-        ++k;
     }
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-        const int c = lane + 32 * i;
-        if (c < cnt && !((unused >> i) & 1u)) tag[cand[c]] = t[i];
-    }
+    for (int i = 0; i < R; ++i)
+        if (pb[i] >= 0) {
+            const int row = cand[lane + 32 * i];
+            const int kk = __popcll(pmask & ((1ull << pb[i]) - 1));
+            bits[kk] = pb[i];
+            srow[kk] = row;
+            tag[row] = t[i];
+        }
     *pm_out = pmask;
     return k;
 }
@@ -779,6 +820,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             S.coef[t] = tag[S.srow[t]] ^ (1ull << t);
             piv[r + t] = 64 * w + S.bits[t];
             prow[r + t] = S.srow[t];
+            S.prev_srow[t] = S.srow[t];
         }
         const int rem = wc - w;
         // 3. reduced pivot rows from the staged original rows (Rbuf row b:
@@ -906,14 +948,14 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             else
                 update_words(pmask, ysnap, w + 2, 1, ulist, nul);
             __syncthreads();
-            for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
+            for (int t = tid; t < p; t += NT) active[S.prev_srow[t]] = 0;
             const int kn = S.p;
             for (int t = tid; t < kn; t += NT) active[S.srow[t]] = 2;
             have_sel = true;
             cur ^= 1;
         } else {
             update_words(pmask, ysnap, w + 2, 0, ulist, nul);
-            for (int t = tid; t < p; t += NT) active[prow[r + t]] = 0;
+            for (int t = tid; t < p; t += NT) active[S.prev_srow[t]] = 0;
         }
         r += p;
         __syncthreads();
