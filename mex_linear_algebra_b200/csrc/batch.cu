@@ -508,6 +508,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     // the matrix itself in shared memory too when it fits (at n = 2m: m up
     // to about 420 with 110 KB, 650 with 220 KB), else in the CTA's
     // L2-resident scratch
+    const size_t pre_a_bytes = used;  // shared bytes before the matrix: free again for the null basis
     if (used + (size_t)m * wc * 8 <= kBigExtra) A = reinterpret_cast<u64 *>(extra + used);
 
     const u64 *src = in + it.in_off;
@@ -977,6 +978,18 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
 
     // ---- null basis
     const int f = n - r;
+    // its index arrays in the elimination's shared memory when they fit
+    if ((size_t)wc * 8 + ((size_t)r + 2 * (size_t)n + wc + 1) * 4 <= pre_a_bytes) {
+        __syncthreads();
+        u64 *pm_s = reinterpret_cast<u64 *>(extra);
+        int *prow_s = reinterpret_cast<int *>(pm_s + wc);
+        for (int t = tid; t < r; t += NT) prow_s[t] = prow[t];
+        pm = pm_s;
+        prow = prow_s;
+        cmap = prow_s + r;
+        fcol = cmap + n;
+        pbase = fcol + n;
+    }
     for (int W = tid; W < wc; W += NT) pm[W] = 0;
     for (int c = tid; c < n; c += NT) cmap[c] = -1;
     __syncthreads();
