@@ -568,7 +568,9 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     // nibble-table lookups per word, TW words at a time, by warps wfirst ..
     // kWarps - 1 (a named barrier among them when warp 0 is busy elsewhere)
     auto update_words = [&](u64 pmask, const u64 *ysp, int x_begin, int wfirst, const int *ul, int nul) {
-        const int nthr = NT - 32 * wfirst, t0 = tid - 32 * wfirst, nw = kWarps - wfirst, wq = warp - wfirst;
+        // wfirst 1: warps other than 0 and 4 (warp 0's scheduler left to it)
+        const int nw = wfirst ? kWarps - 2 : kWarps, nthr = 32 * nw;
+        const int wq = wfirst ? (warp < 4 ? warp - 1 : warp - 2) : warp, t0 = 32 * wq + lane;
         auto bar = [&]() {
             if (wfirst == 0)
                 __syncthreads();
@@ -946,7 +948,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
             // update words w + 2 .. of this one
             if (warp == 0)
                 select_warp(ysn, ncn);
-            else
+            else if (warp != 4)
                 update_words(pmask, ysnap, w + 2, 1, ulist, nul);
             __syncthreads();
             for (int t = tid; t < p; t += NT) active[S.prev_srow[t]] = 0;
