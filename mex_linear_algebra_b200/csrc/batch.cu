@@ -322,19 +322,21 @@ __device__ __forceinline__ u32 bit_mask(const u64 (&y)[R], int b)
 // nonzero panel word; cnt <= 32 R) by one warp, no block barrier: lane l holds
 // candidates l + 32 i.  Per bit that some candidate holds (the OR of their
 // words: XORs create no other bit), the lowest unused candidate holding it
-// becomes pivot k and is XORed into every other candidate holding the bit,
-// each carrying a 64-bit tag of the pivots folded into it.  A step's critical
-// path is a ballot and a shuffle: which rows hold the next bit is computed
-// from the words before the XOR (the bit flips in the rows that take the
-// pivot where the pivot word has it), and the pivots' bits are recorded in
-// registers and written out at the end.  Writes the pivots' bits, rows and
-// tags; returns the pivot count and the pivot mask.
+// becomes pivot k and is XORed into every other candidate holding the bit.
+// A step's critical path is a ballot and a shuffle: which rows hold the next
+// bit is computed from the words before the XOR (the bit flips in the rows
+// that take the pivot where the pivot word has it), and the pivots' bits are
+// kept in registers and written out at the end.  The pivots' combination
+// tags (which other pivots' original rows make up each reduced pivot row)
+// come from a second elimination over the pivots alone, whose pivot rows are
+// known: p steps of two shuffles, no ballot.  Writes the pivots' bits, rows
+// and tags; returns the pivot count and the pivot mask.
 template <int R>
 __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *ysnap, u64 *tag, int *bits,
                                            int *srow, u64 *pm_out)
 {
     const int lane = threadIdx.x & 31;
-    u64 y[R], t[R];
+    u64 y[R];
     int pb[R];  // the bit a candidate became the pivot of, or -1
     u32 unused = 0;
     u64 orw = 0;
@@ -342,7 +344,6 @@ __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *
     for (int i = 0; i < R; ++i) {
         const int c = lane + 32 * i;
         y[i] = c < cnt ? ysnap[cand[c]] : 0ull;
-        t[i] = 0;
         pb[i] = -1;
         unused |= (c < cnt ? 1u : 0u) << i;
         orw |= y[i];
@@ -365,15 +366,11 @@ __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *
                 const int src = __ffs((int)bal) - 1;
                 const int ib = __ffs((int)cm) - 1;  // meaningful in lane src
                 const u64 yp = __shfl_sync(0xffffffffu, pick_reg<R>(y, ib), src);
-                const u64 tp = __shfl_sync(0xffffffffu, pick_reg<R>(t, ib), src) ^ (1ull << k);
                 const u32 me = lane == src ? (1u << ib) : 0u;
                 const u32 hit = hold & ~me;  // every other candidate holding bit b
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    if ((hit >> i) & 1u) {
-                        y[i] ^= yp;
-                        t[i] ^= tp;
-                    }
+                    if ((hit >> i) & 1u) y[i] ^= yp;
                     if ((me >> i) & 1u) pb[i] = b;
                 }
                 unused &= ~me;
@@ -390,12 +387,29 @@ __device__ __forceinline__ int warp_select(const int *cand, int cnt, const u64 *
 #pragma unroll
     for (int i = 0; i < R; ++i)
         if (pb[i] >= 0) {
-            const int row = cand[lane + 32 * i];
             const int kk = __popcll(pmask & ((1ull << pb[i]) - 1));
             bits[kk] = pb[i];
-            srow[kk] = row;
-            tag[row] = t[i];
+            srow[kk] = cand[lane + 32 * i];
         }
+    __syncwarp();
+    // tags: lane l holds pivots l and l + 32 (original panel words)
+    u64 v0 = lane < k ? ysnap[srow[lane]] : 0ull, v1 = lane + 32 < k ? ysnap[srow[lane + 32]] : 0ull;
+    u64 t0 = 0, t1 = 0;
+    for (int q = 0; q < k; ++q) {
+        const int bq = bits[q];
+        const u64 vq = __shfl_sync(0xffffffffu, q < 32 ? v0 : v1, q & 31);
+        const u64 tq = __shfl_sync(0xffffffffu, q < 32 ? t0 : t1, q & 31) ^ (1ull << q);
+        if (lane != q && ((v0 >> bq) & 1ull)) {
+            v0 ^= vq;
+            t0 ^= tq;
+        }
+        if (lane + 32 != q && ((v1 >> bq) & 1ull)) {
+            v1 ^= vq;
+            t1 ^= tq;
+        }
+    }
+    if (lane < k) tag[srow[lane]] = t0;
+    if (lane + 32 < k) tag[srow[lane + 32]] = t1;
     *pm_out = pmask;
     return k;
 }
