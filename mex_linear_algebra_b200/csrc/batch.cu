@@ -568,8 +568,12 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         int kk;
         if (ncand <= 64)
             kk = warp_select<2>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
+        else if (ncand <= 128)
+            kk = warp_select<4>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
         else if (ncand <= 192)
             kk = warp_select<6>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
+        else if (ncand <= 256)
+            kk = warp_select<8>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
         else
             kk = warp_select<12>(S.cand, ncand, ysp, tag, S.bits, S.srow, &pmk);
         if (lane == 0) {
