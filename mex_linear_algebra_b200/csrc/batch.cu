@@ -8,7 +8,8 @@
 //   small  one warp         its slice of shared memory (13 KB)
 //   mid    128 threads      its slice of shared memory (55 KB)
 //   big    the whole CTA    shared memory (up to ~110 KB) or, when it does
-//          (256 threads)    not fit, the CTA's L2-resident global scratch
+//          (256 threads)    not fit, the CTA's L2-resident global scratch;
+//                           blocked by 64-column panels (process_big_blocked)
 //
 // (two CTAs per SM; the single-matrix fused mode runs the same engines in
 // one CTA of 512 threads with 220 KB)
@@ -464,15 +465,21 @@ __device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dl
 
 // Reduced row echelon form and null basis of a big matrix by the whole CTA,
 // 64 columns at a time (the blocked form of elim.cu inside one CTA):
-//  * pivot selection: per bit of the panel, the first active row holding it
-//    becomes a pivot and is XORed into every other row holding it -- on the
-//    panel words only, each row carrying a 64-bit tag of the pivots folded
-//    into it, so pivot k's reduced row is its original row plus the original
-//    pivot rows of its tag (one barrier per bit);
+//  * pivot selection among the panel's candidate rows (unused, nonzero
+//    panel word) by one warp (warp_select), or, with more than kCandMax
+//    candidates, per bit over all rows in registers of eight warps (one named
+//    barrier per bit) -- on the panel words only, each pivot carrying a
+//    64-bit tag of the pivots folded into it, so pivot k's reduced row is its
+//    original row plus the original pivot rows of its tag.  Any independent
+//    set of pivot rows spanning the panel gives the same reduced echelon
+//    form, hence the same rank and null basis;
 //  * the reduced pivot rows R_k are formed from the staged original rows and
 //    written over them; every other row is updated with 16 nibble-table
-//    lookups per word (tables of the 16 combinations of 4 reduced rows),
-//    a warp per row so that global accesses are contiguous;
+//    lookups per word (tables of the 16 combinations of 4 reduced rows);
+//  * look-ahead: words w and w + 1 of every row are updated first (the new
+//    word w + 1 is the next panel's snapshot), then one warp selects panel
+//    w + 1's pivots while the others update words w + 2 .. over the list of
+//    rows that change;
 //  * null basis: Zt = (Y)^T with Y row c = (R restricted to free columns)^T
 //    row p when c is pivot column p, the unit vector of its free index
 //    otherwise -- three 32x32 shuffle transposes, no per-bit gathers.
