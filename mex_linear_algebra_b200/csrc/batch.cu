@@ -63,7 +63,7 @@ constexpr int kSmallBudget = kSmemTotal / (kThreads / 32);       // 13.75 KB
 // shared memory, so that one CTA's barrier-bound panel steps overlap the
 // other's table updates and transposes
 constexpr int kBatchThreads = 256;
-constexpr int kSmallMaxRows = 160;  // largest m for the warp engine
+constexpr int kSmallMaxRows = 192;  // largest m for the warp engine
 constexpr int kMidMaxRows = 240;    // the 128-thread engine below this m
 constexpr int kBatchSmem = kSmemTotal / (kThreads / kBatchThreads);
 
