@@ -589,11 +589,12 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         }
     };
     // words [x_begin, wc) of every row that is not one of the panel's pivots
-    // take the reduced rows of the pivot bits its panel word holds: 16
-    // nibble-table lookups per word, TW words at a time, by warps wfirst ..
-    // kWarps - 1 (a named barrier among them when warp 0 is busy elsewhere)
+    // (or of the rows listed in ul) take the reduced rows of the pivot bits
+    // its panel word holds: 16 nibble-table lookups per word, TW words at a
+    // time.  wfirst 0: by every warp; wfirst 1: by the warps other than 0 and
+    // 4 (warp 0 selects meanwhile; warp 4 shares its scheduler), with a named
+    // barrier among them.
     auto update_words = [&](u64 pmask, const u64 *ysp, int x_begin, int wfirst, const int *ul, int nul) {
-        // wfirst 1: warps other than 0 and 4 (warp 0's scheduler left to it)
         const int nw = wfirst ? kWarps - 2 : kWarps, nthr = 32 * nw;
         const int wq = wfirst ? (warp < 4 ? warp - 1 : warp - 2) : warp, t0 = 32 * wq + lane;
         auto bar = [&]() {
