@@ -236,9 +236,12 @@ __host__ __device__ inline BigLayout big_layout(long long m, long long n)
     L.ints = o; o += (2 * mn + 2 * n + wc + 2 + 1) / 2 + 1;  // piv, prow, fcol, cmap, pbase
     L.pm = o; o += wc;
     L.active = o; o += (m + 7) / 8;
-    L.rt = o; o += (n * ((mn + 31) / 32) + 1) / 2 + 1;      // R^T, 32-bit words
-    L.q = o; o += (mn * ((n + 31) / 32) + 1) / 2 + 1;       // (R restricted to free columns)
-    L.total = o + 8;
+    // R^T and (R restricted to free columns), 32-bit words, rows padded to
+    // a multiple of 4 words and 16-byte aligned (vector stores)
+    o = (o + 1) & ~1LL;
+    L.rt = o; o += n * ((mn + 127) / 128) * 2;
+    L.q = o; o += mn * ((n + 127) / 128) * 2;
+    L.total = (o + 8 + 1) & ~1LL;  // even: every CTA's scratch stays 16-byte aligned
     return L;
 }
 __host__ __device__ inline long long big_scratch_words(long long m, long long n)
@@ -424,41 +427,56 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 
 // 32x32 bit transposes by warp shuffles over a CTA: dst (cols x rows bits,
 // 32-bit words, pitch dld) = src^T, where src row r, 32-bit word x is
-// srcw(r, x) (rows x cols bits).  A warp takes kTrUnroll consecutive tiles
-// at a time and reads all their source words before the first shuffle, so
-// that the (often L2-resident, index-dependent) reads overlap; dst must not
-// overlap what srcw reads.
-constexpr int kTrUnroll = 8;
-template <int NT, typename F>
-__device__ void cta_transpose(F srcw, int rows, int cols, u32 *dst, long long dld)
+// srcw(r, x) (rows x cols bits); dst must not overlap what srcw reads.  A
+// warp unit is one column tile and four row tiles: each lane ends with four
+// consecutive words of its dst row and stores them together (VEC 16: one
+// 16-byte store, dst 16-byte aligned with dld % 4 == 0; VEC 8: two 8-byte
+// stores, dst 8-byte aligned with dld even), a quarter of the store
+// transactions of one word per tile.  Two units (8 source reads a lane, all
+// issued before the first shuffle) are in flight at a time.  dwords: words
+// of a dst row that may be written.
+template <int NT, int VEC, typename F>
+__device__ void cta_transpose4(F srcw, int rows, int cols, u32 *dst, long long dld, int dwords)
 {
-    constexpr int kWarps = NT / 32;
+    constexpr int kWarps = NT / 32, UPI = 2;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5;
-    const long long total = (long long)rt * ct;
-    for (long long t0 = (long long)warp * kTrUnroll; t0 < total; t0 += (long long)kWarps * kTrUnroll) {
-        const int tr0 = (int)(t0 / ct), tc0 = (int)(t0 - (long long)tr0 * ct);
-        int tr[kTrUnroll], tc[kTrUnroll];
-        u32 v[kTrUnroll];
+    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5, rg = (rt + 3) >> 2;
+    const int total = ct * rg;
+    for (int u0 = warp * UPI; u0 < total; u0 += kWarps * UPI) {
+        u32 v[UPI][4];
+        int tc[UPI], g[UPI];
 #pragma unroll
-        for (int u = 0; u < kTrUnroll; ++u) {
-            // tile t0 + u, stepping along the tile row
-            tc[u] = tc0 + u;
-            tr[u] = tr0;
-            while (tc[u] >= ct) {
-                tc[u] -= ct;
-                ++tr[u];
+        for (int u = 0; u < UPI; ++u) {
+            const int unit = u0 + u;
+            g[u] = unit / ct;
+            tc[u] = unit - g[u] * ct;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = (4 * g[u] + i) * 32 + lane;
+                v[u][i] = (unit < total && r < rows) ? srcw(r, tc[u]) : 0u;
             }
-            const int r = tr[u] * 32 + lane;
-            v[u] = (t0 + u < total && r < rows) ? srcw(r, tc[u]) : 0u;
         }
 #pragma unroll
-        for (int u = 0; u < kTrUnroll; ++u) {
-            if (t0 + u >= total) break;  // warp-uniform
-            // lane l gets column tc*32 + l, bit b = row tr*32 + b
-            const u32 keep = transpose32_warp(v[u]);
+        for (int u = 0; u < UPI; ++u) {
+            if (u0 + u >= total) break;  // warp-uniform
+            u32 o[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i] = transpose32_warp(v[u][i]);
             const int c = tc[u] * 32 + lane;
-            if (c < cols) dst[(long long)c * dld + tr[u]] = keep;
+            if (c < cols) {
+                u32 *d = dst + (long long)c * dld + 4 * g[u];
+                const int left = dwords - 4 * g[u];
+                if (VEC == 16 && left >= 4) {
+                    *reinterpret_cast<uint4 *>(d) = make_uint4(o[0], o[1], o[2], o[3]);
+                } else if (VEC == 8 && left >= 4) {
+                    reinterpret_cast<uint2 *>(d)[0] = make_uint2(o[0], o[1]);
+                    reinterpret_cast<uint2 *>(d)[1] = make_uint2(o[2], o[3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (i < left) d[i] = o[i];
+                }
+            }
         }
     }
 }
@@ -1051,16 +1069,17 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     }
     __syncthreads();
     if (f == 0) return;
-    const int rt32 = (r + 31) >> 5, q32 = (f + 31) >> 5;
+    // row pitches of Rt and Q: multiples of 4 words (their scratch is laid out so)
+    const int rt32 = ((r + 127) >> 7) << 2, q32 = ((f + 127) >> 7) << 2;
     if (r > 0) {
         // Rt (n x r) = R^T, R row p = A[prow[p]]
-        cta_transpose<NT>([&](int row, int x) -> u32 {
+        cta_transpose4<NT, 16>([&](int row, int x) -> u32 {
             return reinterpret_cast<const u32 *>(A + (size_t)prow[row] * wc)[x];
-        }, r, n, Rt, rt32);
+        }, r, n, Rt, rt32, rt32);
         __syncthreads();
         // Q (r x f) = (rows f_i of Rt)^T: row p = RREF row p at the free columns
-        cta_transpose<NT>([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
-                      f, r, Q, q32);
+        cta_transpose4<NT, 16>([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
+                               f, r, Q, q32, q32);
         __syncthreads();
     }
     // Zt (f x n) = Y^T, Y row c = Q row p (pivot column c) or e_i (free column i)
@@ -1068,12 +1087,12 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u32 *Z32 = reinterpret_cast<u32 *>(Z);
     if ((n & 63) && (n & 63) <= 32)
         for (int i = tid; i < f; i += NT) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
-    cta_transpose<NT>([&](int c, int y) -> u32 {
+    cta_transpose4<NT, 8>([&](int c, int y) -> u32 {
         const int mc = cmap[c];
         if (mc >= 0) return Q[(long long)mc * q32 + y];
         const int fi = -mc - 1;
         return ((fi >> 5) == y) ? (1u << (fi & 31)) : 0u;
-    }, n, f, Z32, 2LL * wc);
+    }, n, f, Z32, 2LL * wc, (n + 31) >> 5);
     __syncthreads();
 }
 
