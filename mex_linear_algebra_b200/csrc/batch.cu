@@ -1087,12 +1087,17 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u32 *Z32 = reinterpret_cast<u32 *>(Z);
     if ((n & 63) && (n & 63) <= 32)
         for (int i = tid; i < f; i += NT) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
-    cta_transpose4<NT, 8>([&](int c, int y) -> u32 {
+    auto yrow = [&](int c, int y) -> u32 {
         const int mc = cmap[c];
         if (mc >= 0) return Q[(long long)mc * q32 + y];
         const int fi = -mc - 1;
         return ((fi >> 5) == y) ? (1u << (fi & 31)) : 0u;
-    }, n, f, Z32, 2LL * wc, (n + 31) >> 5);
+    };
+    // 16-byte stores where the rows of Zt are 16-byte aligned (even word count)
+    if ((wc & 1) == 0 && (reinterpret_cast<uintptr_t>(Z32) & 15) == 0)
+        cta_transpose4<NT, 16>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
+    else
+        cta_transpose4<NT, 8>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
     __syncthreads();
 }
 
