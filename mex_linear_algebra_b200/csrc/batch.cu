@@ -432,40 +432,34 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 // consecutive words of its dst row and stores them together (VEC 16: one
 // 16-byte store, dst 16-byte aligned with dld % 4 == 0; VEC 8: two 8-byte
 // stores, dst 8-byte aligned with dld even), a quarter of the store
-// transactions of one word per tile.  Two units (8 source reads a lane, all
-// issued before the first shuffle) are in flight at a time.  dwords: words
-// of a dst row that may be written.
+// transactions of one word per tile.  A unit spans two column tiles, read
+// as 64-bit word pairs (srcw2(r, x2) = 32-bit words 2 x2 and 2 x2 + 1 of src
+// row r; four reads a lane, all issued before the first shuffle).  dwords:
+// words of a dst row that may be written.
 template <int NT, int VEC, typename F>
-__device__ void cta_transpose4(F srcw, int rows, int cols, u32 *dst, long long dld, int dwords)
+__device__ void cta_transpose4(F srcw2, int rows, int cols, u32 *dst, long long dld, int dwords)
 {
-    constexpr int kWarps = NT / 32, UPI = 2;
+    constexpr int kWarps = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5, rg = (rt + 3) >> 2;
-    const int total = ct * rg;
-    for (int u0 = warp * UPI; u0 < total; u0 += kWarps * UPI) {
-        u32 v[UPI][4];
-        int tc[UPI], g[UPI];
+    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5, rg = (rt + 3) >> 2, cp = (ct + 1) >> 1;
+    const int total = cp * rg;
+    for (int unit = warp; unit < total; unit += kWarps) {
+        const int g = unit / cp, tcp = unit - g * cp;
+        u64 v[4];
 #pragma unroll
-        for (int u = 0; u < UPI; ++u) {
-            const int unit = u0 + u;
-            g[u] = unit / ct;
-            tc[u] = unit - g[u] * ct;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int r = (4 * g[u] + i) * 32 + lane;
-                v[u][i] = (unit < total && r < rows) ? srcw(r, tc[u]) : 0u;
-            }
+        for (int i = 0; i < 4; ++i) {
+            const int r = (4 * g + i) * 32 + lane;
+            v[i] = r < rows ? srcw2(r, tcp) : 0ull;
         }
 #pragma unroll
-        for (int u = 0; u < UPI; ++u) {
-            if (u0 + u >= total) break;  // warp-uniform
+        for (int h = 0; h < 2; ++h) {
             u32 o[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) o[i] = transpose32_warp(v[u][i]);
-            const int c = tc[u] * 32 + lane;
+            for (int i = 0; i < 4; ++i) o[i] = transpose32_warp((u32)(v[i] >> (32 * h)));
+            const int c = (2 * tcp + h) * 32 + lane;
             if (c < cols) {
-                u32 *d = dst + (long long)c * dld + 4 * g[u];
-                const int left = dwords - 4 * g[u];
+                u32 *d = dst + (long long)c * dld + 4 * g;
+                const int left = dwords - 4 * g;
                 if (VEC == 16 && left >= 4) {
                     *reinterpret_cast<uint4 *>(d) = make_uint4(o[0], o[1], o[2], o[3]);
                 } else if (VEC == 8 && left >= 4) {
@@ -1073,13 +1067,13 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     const int rt32 = ((r + 127) >> 7) << 2, q32 = ((f + 127) >> 7) << 2;
     if (r > 0) {
         // Rt (n x r) = R^T, R row p = A[prow[p]]
-        cta_transpose4<NT, 16>([&](int row, int x) -> u32 {
-            return reinterpret_cast<const u32 *>(A + (size_t)prow[row] * wc)[x];
-        }, r, n, Rt, rt32, rt32);
+        cta_transpose4<NT, 16>([&](int row, int x2) -> u64 { return A[(size_t)prow[row] * wc + x2]; },
+                               r, n, Rt, rt32, rt32);
         __syncthreads();
         // Q (r x f) = (rows f_i of Rt)^T: row p = RREF row p at the free columns
-        cta_transpose4<NT, 16>([&](int row, int x) -> u32 { return Rt[(long long)fcol[row] * rt32 + x]; },
-                               f, r, Q, q32, q32);
+        cta_transpose4<NT, 16>([&](int row, int x2) -> u64 {
+            return reinterpret_cast<const u64 *>(Rt + (long long)fcol[row] * rt32)[x2];
+        }, f, r, Q, q32, q32);
         __syncthreads();
     }
     // Zt (f x n) = Y^T, Y row c = Q row p (pivot column c) or e_i (free column i)
@@ -1087,11 +1081,11 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u32 *Z32 = reinterpret_cast<u32 *>(Z);
     if ((n & 63) && (n & 63) <= 32)
         for (int i = tid; i < f; i += NT) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
-    auto yrow = [&](int c, int y) -> u32 {
+    auto yrow = [&](int c, int y2) -> u64 {
         const int mc = cmap[c];
-        if (mc >= 0) return Q[(long long)mc * q32 + y];
+        if (mc >= 0) return reinterpret_cast<const u64 *>(Q + (long long)mc * q32)[y2];
         const int fi = -mc - 1;
-        return ((fi >> 5) == y) ? (1u << (fi & 31)) : 0u;
+        return ((fi >> 6) == y2) ? (1ull << (fi & 63)) : 0ull;
     };
     // 16-byte stores where the rows of Zt are 16-byte aligned (even word count)
     if ((wc & 1) == 0 && (reinterpret_cast<uintptr_t>(Z32) & 15) == 0)
