@@ -432,31 +432,41 @@ __device__ __forceinline__ u64 sel4r(const u64 (&v)[4], int i)
 // consecutive words of its dst row and stores them together (VEC 16: one
 // 16-byte store, dst 16-byte aligned with dld % 4 == 0; VEC 8: two 8-byte
 // stores, dst 8-byte aligned with dld even), a quarter of the store
-// transactions of one word per tile.  A unit spans two column tiles, read
-// as 64-bit word pairs (srcw2(r, x2) = 32-bit words 2 x2 and 2 x2 + 1 of src
-// row r; four reads a lane, all issued before the first shuffle).  dwords:
-// words of a dst row that may be written.
-template <int NT, int VEC, typename F>
-__device__ void cta_transpose4(F srcw2, int rows, int cols, u32 *dst, long long dld, int dwords)
+// transactions of one word per tile.  A unit spans CW column tiles, read
+// as CW consecutive 32-bit words of a source row (srcw(r, xg) = words
+// CW xg .. CW xg + CW - 1 of src row r, from one 8- or 16-byte load; four
+// reads a lane, all issued before the first shuffle).  dwords: words of a
+// dst row that may be written.
+template <int CW>
+struct TrWords {
+    u32 w[CW];
+};
+template <int NT, int VEC, int CW, typename F>
+__device__ void cta_transpose4(F srcw, int rows, int cols, u32 *dst, long long dld, int dwords)
 {
     constexpr int kWarps = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5, rg = (rt + 3) >> 2, cp = (ct + 1) >> 1;
-    const int total = cp * rg;
+    const int rt = (rows + 31) >> 5, ct = (cols + 31) >> 5, rg = (rt + 3) >> 2, cg = (ct + CW - 1) / CW;
+    const int total = cg * rg;
     for (int unit = warp; unit < total; unit += kWarps) {
-        const int g = unit / cp, tcp = unit - g * cp;
-        u64 v[4];
+        const int g = unit / cg, tcg = unit - g * cg;
+        TrWords<CW> v[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int r = (4 * g + i) * 32 + lane;
-            v[i] = r < rows ? srcw2(r, tcp) : 0ull;
+            if (r < rows) {
+                v[i] = srcw(r, tcg);
+            } else {
+#pragma unroll
+                for (int h = 0; h < CW; ++h) v[i].w[h] = 0u;
+            }
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < CW; ++h) {
             u32 o[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) o[i] = transpose32_warp((u32)(v[i] >> (32 * h)));
-            const int c = (2 * tcp + h) * 32 + lane;
+            for (int i = 0; i < 4; ++i) o[i] = transpose32_warp(v[i].w[h]);
+            const int c = (CW * tcg + h) * 32 + lane;
             if (c < cols) {
                 u32 *d = dst + (long long)c * dld + 4 * g;
                 const int left = dwords - 4 * g;
@@ -473,6 +483,17 @@ __device__ void cta_transpose4(F srcw2, int rows, int cols, u32 *dst, long long 
             }
         }
     }
+}
+// CW consecutive 32-bit words of a row from 8- or 16-byte loads
+__device__ __forceinline__ TrWords<2> tr_words2(const u32 *p)
+{
+    const uint2 x = *reinterpret_cast<const uint2 *>(p);
+    return {{x.x, x.y}};
+}
+__device__ __forceinline__ TrWords<4> tr_words4(const u32 *p)
+{
+    const uint4 x = *reinterpret_cast<const uint4 *>(p);
+    return {{x.x, x.y, x.z, x.w}};
 }
 
 // Reduced row echelon form and null basis of a big matrix by the whole CTA,
@@ -1067,13 +1088,17 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     const int rt32 = ((r + 127) >> 7) << 2, q32 = ((f + 127) >> 7) << 2;
     if (r > 0) {
         // Rt (n x r) = R^T, R row p = A[prow[p]]
-        cta_transpose4<NT, 16>([&](int row, int x2) -> u64 { return A[(size_t)prow[row] * wc + x2]; },
-                               r, n, Rt, rt32, rt32);
+        const u32 *A32 = reinterpret_cast<const u32 *>(A);
+        if ((wc & 1) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0)
+            cta_transpose4<NT, 16, 4>([&](int row, int xg) { return tr_words4(A32 + ((size_t)prow[row] * wc + 2 * xg) * 2); },
+                                      r, n, Rt, rt32, rt32);
+        else
+            cta_transpose4<NT, 16, 2>([&](int row, int xg) { return tr_words2(A32 + ((size_t)prow[row] * wc + xg) * 2); },
+                                      r, n, Rt, rt32, rt32);
         __syncthreads();
         // Q (r x f) = (rows f_i of Rt)^T: row p = RREF row p at the free columns
-        cta_transpose4<NT, 16>([&](int row, int x2) -> u64 {
-            return reinterpret_cast<const u64 *>(Rt + (long long)fcol[row] * rt32)[x2];
-        }, f, r, Q, q32, q32);
+        cta_transpose4<NT, 16, 4>([&](int row, int xg) { return tr_words4(Rt + (long long)fcol[row] * rt32 + 4 * xg); },
+                                  f, r, Q, q32, q32);
         __syncthreads();
     }
     // Zt (f x n) = Y^T, Y row c = Q row p (pivot column c) or e_i (free column i)
@@ -1081,17 +1106,21 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
     u32 *Z32 = reinterpret_cast<u32 *>(Z);
     if ((n & 63) && (n & 63) <= 32)
         for (int i = tid; i < f; i += NT) Z32[(long long)i * 2 * wc + 2 * wc - 1] = 0;
-    auto yrow = [&](int c, int y2) -> u64 {
+    auto yrow = [&](int c, int yg) -> TrWords<4> {
         const int mc = cmap[c];
-        if (mc >= 0) return reinterpret_cast<const u64 *>(Q + (long long)mc * q32)[y2];
-        const int fi = -mc - 1;
-        return ((fi >> 6) == y2) ? (1ull << (fi & 63)) : 0ull;
+        if (mc >= 0) return tr_words4(Q + (long long)mc * q32 + 4 * yg);
+        const int fi = -mc - 1;  // the unit row of free index fi
+        TrWords<4> u{{0u, 0u, 0u, 0u}};
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+            if ((fi >> 5) == 4 * yg + h) u.w[h] = 1u << (fi & 31);
+        return u;
     };
     // 16-byte stores where the rows of Zt are 16-byte aligned (even word count)
     if ((wc & 1) == 0 && (reinterpret_cast<uintptr_t>(Z32) & 15) == 0)
-        cta_transpose4<NT, 16>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
+        cta_transpose4<NT, 16, 4>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
     else
-        cta_transpose4<NT, 8>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
+        cta_transpose4<NT, 8, 4>(yrow, n, f, Z32, 2LL * wc, (n + 31) >> 5);
     __syncthreads();
 }
 
