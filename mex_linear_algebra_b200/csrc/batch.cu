@@ -680,6 +680,43 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                 for (int q = 0; q < 4; ++q) a[q] = y[q] ? A[(size_t)jr[q] * wc + x] : 0ull;
             };
             int jb = wq * 4 * RPW + 4 * hsel;
+            if (ul) {
+                // listed rows (all to update): their words two steps ahead;
+                // coefficient words read from shared memory at use
+                auto load = [&](int j0, int (&jr)[4], u64 (&a)[4]) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) jr[q] = (j0 + q < nul && x < wc) ? ul[j0 + q] : -1;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) a[q] = jr[q] >= 0 ? A[(size_t)jr[q] * wc + x] : 0ull;
+                };
+                int j0r[4], j1r[4];
+                u64 a0[4], a1[4];
+                load(jb, j0r, a0);
+                load(jb + kStep, j1r, a1);
+                for (; jb - 4 * hsel < nul; jb += kStep) {
+                    int j2r[4];
+                    u64 a2[4];
+                    load(jb + 2 * kStep, j2r, a2);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (j0r[q] < 0) continue;
+                        const u64 yq = ysp[j0r[q]] & pmask;
+                        u64 acc = 0;
+#pragma unroll
+                        for (int gi = 0; gi < 16; ++gi) acc ^= S.T[gi][(yq >> (4 * gi)) & 15][xl];
+                        A[(size_t)j0r[q] * wc + x] = a0[q] ^ acc;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        j0r[q] = j1r[q];
+                        a0[q] = a1[q];
+                        j1r[q] = j2r[q];
+                        a1[q] = a2[q];
+                    }
+                }
+                bar();
+                continue;
+            }
             int jr[4];
             u64 y[4], a[4];
             fetch(jb, jr, y, a);
