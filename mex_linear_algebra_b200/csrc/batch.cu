@@ -255,7 +255,7 @@ constexpr int kRegRows = 4;        // rows per thread there
 constexpr int kRegWarps = kRegThreads / 32;
 static_assert(kRegWarps == 8, "eight candidate slots");
 constexpr int kRegBar = 6;         // their named barrier
-constexpr int kSubBar = 5;         // warps 1.. while warp 0 selects the next panel's pivots
+constexpr int kSubBar = 5;         // the update warps while warp 0 selects the next panel's pivots
 constexpr int kCandMax = 384;      // candidate rows one warp selects pivots among (12 a lane)
 template <int TW>
 struct BigSmem {
@@ -1041,7 +1041,8 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         __syncthreads();
         if (ncn <= kCandMax) {
             // 4b. the next panel's pivots by warp 0 while the other warps
-            // update words w + 2 .. of this one
+            // (but warp 4, which shares warp 0's scheduler) update words
+            // w + 2 .. of this one
             if (warp == 0)
                 select_warp(ysn, ncn);
             else if (warp != 4)
