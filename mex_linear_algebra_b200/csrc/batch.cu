@@ -980,6 +980,7 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
         }
         __syncthreads();
         int nc = 0, nu = 0;
+        u32 ub[4] = {0u, 0u, 0u, 0u};  // which rows of the warp's first 128 to update
         for (int j0 = jlo; j0 < jhi; j0 += 128) {
             u64 a1[4];
             int st[4];
@@ -1012,7 +1013,9 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                     upd = y != 0;
                 }
                 nc += __popc(__ballot_sync(0xffffffffu, ok));
-                nu += __popc(__ballot_sync(0xffffffffu, upd));
+                const u32 bu = __ballot_sync(0xffffffffu, upd);
+                nu += __popc(bu);
+                if (j0 == jlo) ub[u] = bu;
             }
         }
         if (lane == 0) {
@@ -1030,12 +1033,21 @@ __device__ void process_big_blocked(const BatchDevItem &it, const u64 *__restric
                 ubase += q < warp ? c : 0;
                 nul += c;
             }
-            for (int j0 = jlo; j0 < jhi; j0 += 32) {
-                const int j = j0 + lane;
-                const bool upd = j < jhi && active[j] != 2 && (ysnap[j] & pmask) != 0;
-                const u32 bal = __ballot_sync(0xffffffffu, upd);
-                if (upd) ulist[ubase + __popc(bal & ((1u << lane) - 1))] = j;
-                ubase += __popc(bal);
+            if (chunk <= 128) {
+                // from the ballots kept during the pass above
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if ((ub[u] >> lane) & 1u) ulist[ubase + __popc(ub[u] & ((1u << lane) - 1))] = jlo + 32 * u + lane;
+                    ubase += __popc(ub[u]);
+                }
+            } else {
+                for (int j0 = jlo; j0 < jhi; j0 += 32) {
+                    const int j = j0 + lane;
+                    const bool upd = j < jhi && active[j] != 2 && (ysnap[j] & pmask) != 0;
+                    const u32 bal = __ballot_sync(0xffffffffu, upd);
+                    if (upd) ulist[ubase + __popc(bal & ((1u << lane) - 1))] = j;
+                    ubase += __popc(bal);
+                }
             }
         }
         __syncthreads();
